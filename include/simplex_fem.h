@@ -1,0 +1,156 @@
+/*
+ * simplex_fem.h - C ABI of the B200 matrix-free tetrahedral FEM engine.
+ *
+ * The functions below replace the operator / preconditioner / solver
+ * interface that the reference benchmark programs build on deal.II:
+ *
+ *   Operator<dim,Number>            CG/cells_batched/application.cc:1040-1582
+ *                                   DG/cells_batched/application.cc:1156-2858
+ *                                   DG/components_batched/application_helmholtz.cc:434-1765
+ *   MultigridPreconditioner         CG/cells_batched/application_ph.cc:1754-2023
+ *                                   DG/cells_batched/application_phc.cc:3396-3667
+ *   SolverCG + PreconditionMG       CG/cells_batched/application_ph.cc:1949-1980
+ *
+ * Conventions
+ *   - Every function returns an int status: FEM_OK (0) or one of FEM_ERR_*.
+ *     fem_last_error_string() gives the message of the last failure on the
+ *     calling thread.
+ *   - Handles are opaque.  A handle is not thread-safe; use one stream per
+ *     handle at a time.
+ *   - Vector arguments are DEVICE pointers (cudaMalloc'd by the caller or by
+ *     fem_vector_alloc) of the operator's number type (double for FEM_FP64,
+ *     float for FEM_FP32) and length m().  `stream` is a cudaStream_t passed
+ *     as void* (NULL = legacy default stream).
+ *   - The library owns the device memory it allocates for meshes, operators,
+ *     multigrid hierarchies and solvers; the caller owns vectors.
+ *   - Host-copy functions (fem_*_copy_*) write into caller-provided host
+ *     buffers and exist for inspection and testing.
+ */
+#ifndef SIMPLEX_FEM_H
+#define SIMPLEX_FEM_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- status codes ------------------------------------------------------ */
+#define FEM_OK 0
+#define FEM_ERR_ARG 1            /* invalid argument */
+#define FEM_ERR_CUDA 2           /* a CUDA runtime call failed */
+#define FEM_ERR_STATE 3          /* call not valid in the handle's state */
+#define FEM_ERR_NOT_CONVERGED 4  /* iterative solver hit its iteration limit */
+#define FEM_ERR_BREAKDOWN 5      /* CG breakdown: p^T A p <= 0 */
+#define FEM_ERR_NONFINITE 6      /* NaN/Inf met in a residual or dot product */
+#define FEM_ERR_INTERNAL 7
+
+/* ---- enums ------------------------------------------------------------- */
+enum fem_kind {
+  FEM_CG = 0,        /* continuous Lagrange, Laplace, homogeneous Dirichlet (strong) */
+  FEM_DG = 1,        /* discontinuous Lagrange, SIPG Laplace, weak Dirichlet */
+  FEM_HELMHOLTZ = 2  /* DG, n_components fields, mass + SIPG Laplace */
+};
+enum fem_precision { FEM_FP64 = 0, FEM_FP32 = 1 };
+enum fem_penalty {
+  FEM_PENALTY_REFERENCE = 0, /* (p+1)(p+d)/d * surface/volume (DG/cells_batched/application.cc:1193-1245) */
+  FEM_PENALTY_SQUARE = 1     /* (p+1)^2 * surface/volume */
+};
+
+typedef struct fem_mesh fem_mesh;
+typedef struct fem_op fem_op;
+typedef struct fem_batch fem_batch;
+typedef struct fem_mg fem_mg;
+typedef struct fem_mlp fem_mlp;
+
+/* Kuhn-subdivided box: n[0]*n[1]*n[2] hexes x 6 tets, interior vertices
+ * jittered by U[-jitter*h, jitter*h] per axis from std::mt19937_64(seed).
+ * Replaces GridGenerator::subdivided_hyper_cube_with_simplices +
+ * refine_global (CG/cells_batched/application.cc:1762-1770). */
+typedef struct fem_mesh_desc {
+  int32_t n[3];
+  double lo[3];
+  double hi[3];
+  double jitter;
+  uint64_t seed;
+} fem_mesh_desc;
+
+typedef struct fem_op_params {
+  double mass_coefficient; /* FEM_HELMHOLTZ: factor of the mass term (reference: 1e5) */
+  int32_t n_components;    /* FEM_HELMHOLTZ: number of fields (reference: 3); others: 1 */
+  int32_t penalty;         /* FEM_DG: enum fem_penalty */
+  int32_t reserved[6];
+} fem_op_params;
+
+/* ---- library ----------------------------------------------------------- */
+const char* fem_last_error_string(void);
+int fem_version(int32_t* major, int32_t* minor);
+
+/* ---- mesh -------------------------------------------------------------- */
+int fem_mesh_create(const fem_mesh_desc* desc, fem_mesh** out);
+int fem_mesh_destroy(fem_mesh* mesh);
+int fem_mesh_sizes(const fem_mesh* mesh, int64_t* n_vertices, int64_t* n_cells,
+                   int64_t* n_interior_faces, int64_t* n_boundary_faces);
+int fem_mesh_copy_vertices(const fem_mesh* mesh, double* xyz /* [n_vertices][3] */);
+int fem_mesh_copy_cells(const fem_mesh* mesh, int32_t* cell_vertices /* [n_cells][4] */);
+int fem_mesh_copy_neighbors(const fem_mesh* mesh, int32_t* nb /* [n_cells][4] */,
+                            int8_t* nb_face /* [n_cells][4] */);
+
+/* Host-only continuous P_degree numbering of the mesh (first touch in the
+ * hierarchical cell order) and its homogeneous Dirichlet mask; no GPU needed.
+ * Call with cell_dofs == NULL and constrained == NULL to query n_dofs.
+ * Replaces DoFHandler::distribute_dofs + DoFRenumbering::matrix_free_data_locality
+ * + VectorTools::interpolate_boundary_values (CG/cells_batched/application.cc:1809-1838). */
+int fem_mesh_cg_dofs(const fem_mesh* mesh, int32_t degree, int64_t* n_dofs,
+                     int32_t* cell_dofs /* [n_cells][dofs_per_cell] */,
+                     uint8_t* constrained /* [n_dofs] */);
+
+/* ---- operator ------------------------------------------------------------
+ * fem_op_create replaces Operator::reinit (CG/cells_batched/application.cc:1056-1128,
+ * DG/cells_batched/application.cc:1170-1277, application_helmholtz.cc:450-510).
+ * CG operators keep ones on the constrained diagonal (reinit(..., true),
+ * CG/cells_batched/application.cc:1842). */
+int fem_op_create(fem_mesh* mesh, int32_t degree, int32_t kind, int32_t precision,
+                  const fem_op_params* params /* may be NULL */, fem_op** out);
+int fem_op_destroy(fem_op* op);
+/* Operator::m() (CG/cells_batched/application.cc:1131-1139) */
+int fem_op_m(const fem_op* op, uint64_t* m);
+int fem_op_info(const fem_op* op, int32_t* degree, int32_t* kind, int32_t* precision,
+                int32_t* dofs_per_cell, int64_t* n_cells, int32_t* n_components);
+/* CG: global DoF of local node i of cell c, [n_cells][dofs_per_cell];
+ * DG: the identity layout c*n_components*dofs_per_cell + comp*dofs_per_cell + i. */
+int fem_op_copy_dof_map(const fem_op* op, int32_t* cell_dofs);
+int fem_op_copy_constrained(const fem_op* op, uint8_t* mask /* [m] */);
+int fem_op_copy_support_points(const fem_op* op, double* xyz /* [m/n_components][3] */);
+/* Operator::vmult_masked_gather / vmult_manual / vmult
+ * (CG/cells_batched/application.cc:1167-1176, DG/cells_batched/application.cc:1319-1332,
+ * application_helmholtz.cc:567-580): dst = A src.  dst and src must not alias. */
+int fem_op_vmult(fem_op* op, void* dst, const void* src, void* stream);
+/* Operator::Tvmult (CG/cells_batched/application.cc:1193-1197): the operator is symmetric. */
+int fem_op_Tvmult(fem_op* op, void* dst, const void* src, void* stream);
+/* Operator::compute_inverse_diagonal (CG/cells_batched/application_ph.cc:1382-1404):
+ * 1/diag, 1 where |diag| < 1e-10. */
+int fem_op_compute_inverse_diagonal(fem_op* op, void* inv_diag, void* stream);
+/* MatrixFreeTools::compute_diagonal / Operator::get_diagonal
+ * (application_helmholtz.cc:588-600). */
+int fem_op_compute_diagonal(fem_op* op, void* diag, void* stream);
+/* One phase of vmult, for per-kernel timing: CG phase 1 zeroes dst and
+ * phase 2 runs the fused cell kernel; DG/Helmholtz phase 1 publishes the
+ * face normal derivatives and phase 2 runs the fused cell+face kernel.
+ * Running phase 1 then phase 2 equals fem_op_vmult. */
+int fem_op_vmult_phase(fem_op* op, void* dst, const void* src, int32_t phase, void* stream);
+/* Algorithmic work of one vmult: flops and bytes of the fused kernels. */
+int fem_op_work(const fem_op* op, double* flops, double* bytes);
+
+/* ---- batched multi-problem launch (components-batched Helmholtz etc.) ----
+ * All operators must share kind, degree, precision and n_components.  One
+ * persistent launch per phase covers every problem. */
+int fem_batch_create(fem_op* const* ops, int32_t n_ops, fem_batch** out);
+int fem_batch_destroy(fem_batch* batch);
+int fem_batch_vmult(fem_batch* batch, void* const* dst, const void* const* src, void* stream);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* SIMPLEX_FEM_H */

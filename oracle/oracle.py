@@ -1,0 +1,131 @@
+"""ctypes binding of liboracle.so, the CPU restatement used as the checker.
+
+TEST INFRASTRUCTURE ONLY (tests/, __graft_entry__.smoke(), bench.py's CPU
+baseline leg).  See oracle.h for what it restates and its parity status.
+"""
+import ctypes as C
+import os
+import subprocess
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "liboracle.so")
+CG, DG, HELMHOLTZ = 0, 1, 2
+
+
+class Params(C.Structure):
+    _fields_ = [("degree", C.c_int32), ("kind", C.c_int32), ("n_components", C.c_int32),
+                ("penalty", C.c_int32), ("mass", C.c_double), ("quad_points", C.c_int32),
+                ("n_threads", C.c_int32)]
+
+
+_lib = None
+
+
+def build():
+    subprocess.run(["make", "-s", "-C", _HERE], check=True)
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            build()
+        L = C.CDLL(LIB_PATH)
+        L.oracle_create.restype = C.c_int
+        L.oracle_create.argtypes = [C.POINTER(Params), C.c_int64, C.c_void_p, C.c_int64, C.c_void_p,
+                                    C.c_void_p, C.c_void_p, C.c_int64, C.POINTER(C.c_void_p)]
+        L.oracle_destroy.argtypes = [C.c_void_p]
+        L.oracle_vmult.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p]
+        L.oracle_vmult_cells.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_int64, C.c_int64]
+        L.oracle_diagonal.argtypes = [C.c_void_p, C.c_void_p]
+        L.oracle_cell_matrix.argtypes = [C.c_void_p, C.c_int64, C.c_void_p]
+        L.oracle_check_cg_numbering.restype = C.c_int64
+        L.oracle_check_cg_numbering.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p]
+        L.oracle_basis.argtypes = [C.c_int32, C.c_void_p, C.c_void_p, C.c_void_p]
+        L.oracle_n_dofs.restype = C.c_int64
+        L.oracle_n_dofs.argtypes = [C.c_void_p]
+        L.oracle_quadrature_sizes.argtypes = [C.c_void_p, C.POINTER(C.c_int32), C.POINTER(C.c_int32)]
+        _lib = L
+    return _lib
+
+
+class Oracle:
+    """FP64 CPU operator on the same mesh arrays as the product."""
+
+    def __init__(self, x, cells, degree, kind, cell_dofs=None, constrained=None, n_components=1,
+                 penalty=0, mass=1e5, quad_points=0, n_threads=0):
+        self.x = np.ascontiguousarray(x, np.float64)
+        self.cells = np.ascontiguousarray(cells, np.int32)
+        p = Params(degree, kind, n_components, penalty, mass, quad_points, n_threads)
+        self.kind = kind
+        if kind == CG:
+            self.cell_dofs = np.ascontiguousarray(cell_dofs, np.int32)
+            self.constrained = np.ascontiguousarray(constrained, np.uint8)
+            nd = len(self.constrained)
+            cdp, cmp = self.cell_dofs.ctypes.data, self.constrained.ctypes.data
+        else:
+            nd, cdp, cmp = 0, None, None
+        h = C.c_void_p()
+        rc = lib().oracle_create(C.byref(p), len(self.x), self.x.ctypes.data, len(self.cells),
+                                 self.cells.ctypes.data, cdp, cmp, nd, C.byref(h))
+        if rc != 0:
+            raise RuntimeError(f"oracle_create failed: {rc}")
+        self.h = h
+        self.n = lib().oracle_n_dofs(h)
+        self.K = (degree + 1) * (degree + 2) * (degree + 3) // 6
+        self.nc = n_components
+
+    def vmult(self, src):
+        src = np.ascontiguousarray(src, np.float64)
+        dst = np.empty(self.n, np.float64)
+        lib().oracle_vmult(self.h, src.ctypes.data, dst.ctypes.data)
+        return dst
+
+    def vmult_cells(self, src, dst, c0, c1):
+        """Contributions of cells [c0, c1) into dst (a timing sample)."""
+        lib().oracle_vmult_cells(self.h, src.ctypes.data, dst.ctypes.data, c0, c1)
+
+    def diagonal(self):
+        d = np.empty(self.n, np.float64)
+        lib().oracle_diagonal(self.h, d.ctypes.data)
+        return d
+
+    def cell_matrix(self, c):
+        n = self.K * self.nc
+        m = np.empty((n, n), np.float64)
+        lib().oracle_cell_matrix(self.h, c, m.ctypes.data)
+        return m
+
+    def check_cg_numbering(self, lo, hi):
+        lo = np.ascontiguousarray(lo, np.float64)
+        hi = np.ascontiguousarray(hi, np.float64)
+        return lib().oracle_check_cg_numbering(self.h, lo.ctypes.data, hi.ctypes.data)
+
+    def quadrature_sizes(self):
+        a, b = C.c_int32(), C.c_int32()
+        lib().oracle_quadrature_sizes(self.h, C.byref(a), C.byref(b))
+        return a.value, b.value
+
+    def __del__(self):
+        if getattr(self, "h", None) and _lib is not None:
+            _lib.oracle_destroy(self.h)
+            self.h = None
+
+
+def basis(degree, xi):
+    K = (degree + 1) * (degree + 2) * (degree + 3) // 6
+    v = np.empty(K)
+    g = np.empty((K, 3))
+    xi = np.ascontiguousarray(xi, np.float64)
+    lib().oracle_basis(degree, xi.ctypes.data, v.ctypes.data, g.ctypes.data)
+    return v, g
+
+
+def for_mesh(mesh, degree, kind, **kw):
+    """Oracle on a simplexfem.Mesh (CG uses the mesh's own CG numbering)."""
+    if kind == CG:
+        cd, cm = mesh.cg_dofs(degree)
+        return Oracle(mesh.vertices(), mesh.cells(), degree, CG, cell_dofs=cd, constrained=cm, **kw)
+    return Oracle(mesh.vertices(), mesh.cells(), degree, kind, **kw)

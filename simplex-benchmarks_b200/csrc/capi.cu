@@ -1,0 +1,295 @@
+// extern "C" entry points of include/simplex_fem.h.
+#include <cstring>
+#include <memory>
+#include <string>
+#include <vector>
+
+#include "../../include/simplex_fem.h"
+#include "common.hpp"
+#include "mesh.hpp"
+#include "operator.hpp"
+
+struct fem_mesh {
+  sfem::Mesh mesh;
+};
+struct fem_op {
+  std::unique_ptr<sfem::Operator> op;
+};
+struct fem_batch {
+  std::unique_ptr<sfem::Batch> batch;
+};
+
+namespace sfem {
+namespace {
+thread_local std::string g_last_error;
+}
+void set_last_error(const std::string& msg) { g_last_error = msg; }
+const char* last_error() { return g_last_error.c_str(); }
+}  // namespace sfem
+
+namespace {
+template <class F>
+int guarded(F&& f) {
+  try {
+    f();
+    return FEM_OK;
+  } catch (const sfem::Error& e) {
+    sfem::set_last_error(e.what());
+    return e.code;
+  } catch (const std::bad_alloc&) {
+    sfem::set_last_error("host allocation failed");
+    return FEM_ERR_INTERNAL;
+  } catch (const std::exception& e) {
+    sfem::set_last_error(e.what());
+    return FEM_ERR_INTERNAL;
+  }
+}
+#define REQUIRE_PTR(p) SFEM_REQUIRE((p) != nullptr, FEM_ERR_ARG, #p " is NULL")
+}  // namespace
+
+extern "C" {
+
+const char* fem_last_error_string(void) { return sfem::last_error(); }
+
+int fem_version(int32_t* major, int32_t* minor) {
+  return guarded([&] {
+    REQUIRE_PTR(major);
+    REQUIRE_PTR(minor);
+    *major = 0;
+    *minor = 1;
+  });
+}
+
+int fem_mesh_create(const fem_mesh_desc* desc, fem_mesh** out) {
+  return guarded([&] {
+    REQUIRE_PTR(desc);
+    REQUIRE_PTR(out);
+    sfem::MeshDescription d;
+    for (int a = 0; a < 3; ++a) {
+      d.n[a] = desc->n[a];
+      d.lo[a] = desc->lo[a];
+      d.hi[a] = desc->hi[a];
+    }
+    d.jitter = desc->jitter;
+    d.seed = desc->seed;
+    auto m = std::make_unique<fem_mesh>();
+    m->mesh = sfem::build_kuhn_mesh(d);
+    *out = m.release();
+  });
+}
+
+int fem_mesh_destroy(fem_mesh* mesh) {
+  return guarded([&] { delete mesh; });
+}
+
+int fem_mesh_sizes(const fem_mesh* mesh, int64_t* n_vertices, int64_t* n_cells, int64_t* n_interior_faces,
+                   int64_t* n_boundary_faces) {
+  return guarded([&] {
+    REQUIRE_PTR(mesh);
+    if (n_vertices) *n_vertices = mesh->mesh.n_vertices;
+    if (n_cells) *n_cells = mesh->mesh.n_cells;
+    if (n_interior_faces) *n_interior_faces = mesh->mesh.n_interior_faces;
+    if (n_boundary_faces) *n_boundary_faces = mesh->mesh.n_boundary_faces;
+  });
+}
+
+int fem_mesh_copy_vertices(const fem_mesh* mesh, double* xyz) {
+  return guarded([&] {
+    REQUIRE_PTR(mesh);
+    REQUIRE_PTR(xyz);
+    std::memcpy(xyz, mesh->mesh.x.data(), mesh->mesh.x.size() * sizeof(double));
+  });
+}
+
+int fem_mesh_copy_cells(const fem_mesh* mesh, int32_t* cells) {
+  return guarded([&] {
+    REQUIRE_PTR(mesh);
+    REQUIRE_PTR(cells);
+    std::memcpy(cells, mesh->mesh.cell_vertices.data(), mesh->mesh.cell_vertices.size() * sizeof(int32_t));
+  });
+}
+
+int fem_mesh_copy_neighbors(const fem_mesh* mesh, int32_t* nb, int8_t* nbf) {
+  return guarded([&] {
+    REQUIRE_PTR(mesh);
+    if (nb) std::memcpy(nb, mesh->mesh.nb.data(), mesh->mesh.nb.size() * sizeof(int32_t));
+    if (nbf) std::memcpy(nbf, mesh->mesh.nbf.data(), mesh->mesh.nbf.size() * sizeof(int8_t));
+  });
+}
+
+int fem_mesh_cg_dofs(const fem_mesh* mesh, int32_t degree, int64_t* n_dofs, int32_t* cell_dofs,
+                     uint8_t* constrained) {
+  return guarded([&] {
+    REQUIRE_PTR(mesh);
+    REQUIRE_PTR(n_dofs);
+    sfem::CGDofs d = sfem::build_cg_dofs(mesh->mesh, degree);
+    *n_dofs = d.n_dofs;
+    if (cell_dofs) std::memcpy(cell_dofs, d.cell_dofs.data(), d.cell_dofs.size() * sizeof(int32_t));
+    if (constrained) std::memcpy(constrained, d.constrained.data(), d.constrained.size());
+  });
+}
+
+int fem_op_create(fem_mesh* mesh, int32_t degree, int32_t kind, int32_t precision, const fem_op_params* params,
+                  fem_op** out) {
+  return guarded([&] {
+    REQUIRE_PTR(mesh);
+    REQUIRE_PTR(out);
+    sfem::OpConfig cfg;
+    cfg.degree = degree;
+    cfg.kind = kind;
+    cfg.precision = precision;
+    if (kind == FEM_HELMHOLTZ) {
+      cfg.mass = 1e5;
+      cfg.n_components = 3;
+    }
+    if (params) {
+      if (kind == FEM_HELMHOLTZ) {
+        cfg.mass = params->mass_coefficient;
+        cfg.n_components = params->n_components > 0 ? params->n_components : 3;
+      }
+      cfg.penalty = params->penalty;
+      SFEM_REQUIRE(cfg.penalty == FEM_PENALTY_REFERENCE || cfg.penalty == FEM_PENALTY_SQUARE, FEM_ERR_ARG,
+                   "penalty must be FEM_PENALTY_REFERENCE or FEM_PENALTY_SQUARE");
+    }
+    auto o = std::make_unique<fem_op>();
+    o->op = sfem::make_operator(mesh->mesh, cfg);
+    *out = o.release();
+  });
+}
+
+int fem_op_destroy(fem_op* op) {
+  return guarded([&] { delete op; });
+}
+
+int fem_op_m(const fem_op* op, uint64_t* m) {
+  return guarded([&] {
+    REQUIRE_PTR(op);
+    REQUIRE_PTR(m);
+    *m = uint64_t(op->op->m);
+  });
+}
+
+int fem_op_info(const fem_op* op, int32_t* degree, int32_t* kind, int32_t* precision, int32_t* dofs_per_cell,
+                int64_t* n_cells, int32_t* n_components) {
+  return guarded([&] {
+    REQUIRE_PTR(op);
+    const auto& o = *op->op;
+    if (degree) *degree = o.cfg.degree;
+    if (kind) *kind = o.cfg.kind;
+    if (precision) *precision = o.cfg.precision;
+    if (dofs_per_cell) *dofs_per_cell = o.K;
+    if (n_cells) *n_cells = o.n_cells;
+    if (n_components) *n_components = o.cfg.n_components;
+  });
+}
+
+int fem_op_copy_dof_map(const fem_op* op, int32_t* cell_dofs) {
+  return guarded([&] {
+    REQUIRE_PTR(op);
+    REQUIRE_PTR(cell_dofs);
+    const auto& o = *op->op;
+    if (o.cfg.kind == FEM_CG) {
+      std::memcpy(cell_dofs, o.cell_dofs.data(), o.cell_dofs.size() * sizeof(int32_t));
+    } else {
+      const int64_t nk = int64_t(o.K) * o.cfg.n_components;
+      for (int64_t c = 0; c < o.n_cells; ++c)
+        for (int64_t i = 0; i < nk; ++i) cell_dofs[c * nk + i] = int32_t(c * nk + i);
+    }
+  });
+}
+
+int fem_op_copy_constrained(const fem_op* op, uint8_t* mask) {
+  return guarded([&] {
+    REQUIRE_PTR(op);
+    REQUIRE_PTR(mask);
+    std::memcpy(mask, op->op->constrained.data(), op->op->constrained.size());
+  });
+}
+
+int fem_op_copy_support_points(const fem_op* op, double* xyz) {
+  return guarded([&] {
+    REQUIRE_PTR(op);
+    REQUIRE_PTR(xyz);
+    std::memcpy(xyz, op->op->support.data(), op->op->support.size() * sizeof(double));
+  });
+}
+
+int fem_op_vmult(fem_op* op, void* dst, const void* src, void* stream) {
+  return guarded([&] {
+    REQUIRE_PTR(op);
+    REQUIRE_PTR(dst);
+    REQUIRE_PTR(src);
+    SFEM_REQUIRE(dst != src, FEM_ERR_ARG, "vmult: dst and src must not alias");
+    op->op->vmult(dst, src, static_cast<cudaStream_t>(stream));
+  });
+}
+
+int fem_op_vmult_phase(fem_op* op, void* dst, const void* src, int32_t phase, void* stream) {
+  return guarded([&] {
+    REQUIRE_PTR(op);
+    REQUIRE_PTR(dst);
+    REQUIRE_PTR(src);
+    SFEM_REQUIRE(phase == 1 || phase == 2, FEM_ERR_ARG, "vmult_phase: phase must be 1 or 2");
+    op->op->vmult_phase(dst, src, phase, static_cast<cudaStream_t>(stream));
+  });
+}
+
+int fem_op_Tvmult(fem_op* op, void* dst, const void* src, void* stream) {
+  return fem_op_vmult(op, dst, src, stream);
+}
+
+int fem_op_compute_inverse_diagonal(fem_op* op, void* diag, void* stream) {
+  return guarded([&] {
+    REQUIRE_PTR(op);
+    REQUIRE_PTR(diag);
+    op->op->inverse_diagonal(diag, static_cast<cudaStream_t>(stream));
+  });
+}
+
+int fem_op_compute_diagonal(fem_op* op, void* diag, void* stream) {
+  return guarded([&] {
+    REQUIRE_PTR(op);
+    REQUIRE_PTR(diag);
+    op->op->diagonal(diag, static_cast<cudaStream_t>(stream));
+  });
+}
+
+int fem_op_work(const fem_op* op, double* flops, double* bytes) {
+  return guarded([&] {
+    REQUIRE_PTR(op);
+    double f = 0, b = 0;
+    op->op->work(f, b);
+    if (flops) *flops = f;
+    if (bytes) *bytes = b;
+  });
+}
+
+int fem_batch_create(fem_op* const* ops, int32_t n_ops, fem_batch** out) {
+  return guarded([&] {
+    REQUIRE_PTR(ops);
+    REQUIRE_PTR(out);
+    std::vector<sfem::Operator*> v;
+    for (int i = 0; i < n_ops; ++i) {
+      REQUIRE_PTR(ops[i]);
+      v.push_back(ops[i]->op.get());
+    }
+    auto b = std::make_unique<fem_batch>();
+    b->batch = sfem::make_batch(v);
+    *out = b.release();
+  });
+}
+
+int fem_batch_destroy(fem_batch* batch) {
+  return guarded([&] { delete batch; });
+}
+
+int fem_batch_vmult(fem_batch* batch, void* const* dst, const void* const* src, void* stream) {
+  return guarded([&] {
+    REQUIRE_PTR(batch);
+    REQUIRE_PTR(dst);
+    REQUIRE_PTR(src);
+    batch->batch->vmult(dst, src, static_cast<cudaStream_t>(stream));
+  });
+}
+
+}  // extern "C"

@@ -1,0 +1,34 @@
+// Shared host-side utilities: error reporting and checked CUDA calls.
+#pragma once
+#include <cstdint>
+#include <stdexcept>
+#include <string>
+
+namespace sfem {
+
+// Error raised anywhere below the C ABI; converted to a status code plus a
+// message readable through fem_last_error_string().
+struct Error : std::runtime_error {
+  int code;
+  Error(int c, const std::string& m) : std::runtime_error(m), code(c) {}
+};
+
+void set_last_error(const std::string& msg);
+const char* last_error();
+
+}  // namespace sfem
+
+#define SFEM_REQUIRE(cond, code, msg)                                   \
+  do {                                                                  \
+    if (!(cond)) throw ::sfem::Error((code), std::string(msg));         \
+  } while (0)
+
+#ifdef __CUDACC__
+#include <cuda_runtime.h>
+#define SFEM_CUDA(call)                                                                   \
+  do {                                                                                    \
+    cudaError_t e_ = (call);                                                              \
+    if (e_ != cudaSuccess)                                                                \
+      throw ::sfem::Error(FEM_ERR_CUDA, std::string(#call) + ": " + cudaGetErrorString(e_)); \
+  } while (0)
+#endif

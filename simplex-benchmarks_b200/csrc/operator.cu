@@ -1,0 +1,366 @@
+// Operator set-up (geometry, penalties, index tables) and kernel dispatch.
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+
+#include "kernels_cg.cuh"
+#include "kernels_dg.cuh"
+#include "operator.hpp"
+#include "ref_tables.h"
+
+namespace sfem {
+
+namespace {
+
+template <typename T>
+__global__ void inverse_diagonal_kernel(int64_t n, T* d) {
+  const int64_t i = blockIdx.x * int64_t(blockDim.x) + threadIdx.x;
+  if (i < n) {
+    const T v = d[i];
+    d[i] = fabs(double(v)) > 1e-10 ? T(1) / v : T(1);
+  }
+}
+
+inline unsigned blocks_for(int64_t n, int bs) { return unsigned((n + bs - 1) / bs); }
+
+template <int P>
+int nnz_grad() {
+  int z = 0;
+  using Tb = ref::Tables<P>;
+  for (int a = 0; a < 3; ++a)
+    for (int m = 0; m < Tb::KQ; ++m)
+      for (int i = 0; i < Tb::K; ++i) z += Tb::D[a][m][i] != 0.0;
+  return z;
+}
+int nnz_grad_rt(int p) { return p == 1 ? nnz_grad<1>() : p == 2 ? nnz_grad<2>() : nnz_grad<3>(); }
+int kq_of(int p) { return p == 1 ? 1 : p == 2 ? 4 : 10; }
+int k_of(int p) { return (p + 1) * (p + 2) * (p + 3) / 6; }
+int nf_of(int p) { return (p + 1) * (p + 2) / 2; }
+int nfq_of(int p) { return p == 1 ? 1 : p * (p + 1) / 2; }
+
+// metric G = |det J| J^-1 J^-T as (00,11,22,01,02,12)
+void metric(const CellGeometry& g, double G[6]) {
+  const double ad = std::fabs(g.det);
+  auto mm = [&](int a, int b) {
+    double s = 0;
+    for (int c = 0; c < 3; ++c) s += g.Jinv[a][c] * g.Jinv[b][c];
+    return ad * s;
+  };
+  G[0] = mm(0, 0); G[1] = mm(1, 1); G[2] = mm(2, 2);
+  G[3] = mm(0, 1); G[4] = mm(0, 2); G[5] = mm(1, 2);
+}
+
+// ------------------------------------------------------------------ CG ----
+template <typename T>
+class CGOperator final : public Operator {
+ public:
+  DevBuf<int32_t> d_dofs;        // [K][n_cells], -1 = constrained
+  DevBuf<T> d_geo;               // [6][n_cells]
+  DevBuf<int32_t> d_constrained; // constrained DoF list
+
+  CGOperator(const Mesh& mesh, const OpConfig& c) {
+    cfg = c;
+    CGDofs dofs = build_cg_dofs(mesh, cfg.degree);
+    K = dofs.K;
+    n_cells = mesh.n_cells;
+    m = dofs.n_dofs;
+    n_interior_faces = mesh.n_interior_faces;
+    n_boundary_faces = mesh.n_boundary_faces;
+    cell_dofs = dofs.cell_dofs;
+    constrained = dofs.constrained;
+    support = dofs.support;
+    std::vector<int32_t> idx(size_t(K) * n_cells);
+    for (int64_t cc = 0; cc < n_cells; ++cc)
+      for (int i = 0; i < K; ++i) {
+        const int32_t g = dofs.cell_dofs[K * cc + i];
+        idx[size_t(i) * n_cells + cc] = dofs.constrained[g] ? -1 : g;
+      }
+    d_dofs.upload(idx);
+    std::vector<T> geo(6 * size_t(n_cells));
+    for (int64_t cc = 0; cc < n_cells; ++cc) {
+      double G[6];
+      metric(cell_geometry(mesh, cc), G);
+      for (int k = 0; k < 6; ++k) geo[size_t(k) * n_cells + cc] = T(G[k]);
+    }
+    d_geo.upload(geo);
+    std::vector<int32_t> cl;
+    for (int64_t i = 0; i < m; ++i)
+      if (constrained[i]) cl.push_back(int32_t(i));
+    d_constrained.upload(cl);
+  }
+
+  void vmult(void* dst, const void* src, cudaStream_t s) override {
+    vmult_phase(dst, src, 1, s);
+    vmult_phase(dst, src, 2, s);
+  }
+
+  void vmult_phase(void* dst, const void* src, int phase, cudaStream_t s) override {
+    T* d = static_cast<T*>(dst);
+    const T* x = static_cast<const T*>(src);
+    if (phase == 1) {
+      SFEM_CUDA(cudaMemsetAsync(d, 0, sizeof(T) * m, s));
+      return;
+    }
+    const int64_t n = std::max<int64_t>(n_cells, int64_t(d_constrained.n));
+    const unsigned grid = blocks_for(n, 128);
+    switch (cfg.degree) {
+      case 1: cg_cell_kernel<1, T><<<grid, 128, 0, s>>>(n_cells, d_dofs.p, d_geo.p, x, d, d_constrained.n, d_constrained.p); break;
+      case 2: cg_cell_kernel<2, T><<<grid, 128, 0, s>>>(n_cells, d_dofs.p, d_geo.p, x, d, d_constrained.n, d_constrained.p); break;
+      case 3: cg_cell_kernel<3, T><<<grid, 128, 0, s>>>(n_cells, d_dofs.p, d_geo.p, x, d, d_constrained.n, d_constrained.p); break;
+    }
+    SFEM_CUDA(cudaGetLastError());
+  }
+
+  void diagonal(void* diag, cudaStream_t s) override {
+    T* d = static_cast<T*>(diag);
+    SFEM_CUDA(cudaMemsetAsync(d, 0, sizeof(T) * m, s));
+    const int64_t n = std::max<int64_t>(n_cells, int64_t(d_constrained.n));
+    const unsigned grid = blocks_for(n, 128);
+    switch (cfg.degree) {
+      case 1: cg_diagonal_kernel<1, T><<<grid, 128, 0, s>>>(n_cells, d_dofs.p, d_geo.p, d, d_constrained.n, d_constrained.p); break;
+      case 2: cg_diagonal_kernel<2, T><<<grid, 128, 0, s>>>(n_cells, d_dofs.p, d_geo.p, d, d_constrained.n, d_constrained.p); break;
+      case 3: cg_diagonal_kernel<3, T><<<grid, 128, 0, s>>>(n_cells, d_dofs.p, d_geo.p, d, d_constrained.n, d_constrained.p); break;
+    }
+    SFEM_CUDA(cudaGetLastError());
+  }
+
+  void work(double& flops, double& bytes) const override {
+    const int p = cfg.degree, kq = kq_of(p);
+    const double per_cell = 2.0 * (2 * nnz_grad_rt(p) + 9 * kq + 3 * kq * kq);
+    flops = per_cell * double(n_cells);
+    const double s = double(sizeof(T));
+    bytes = 2 * s * double(m) + 4.0 * K * double(n_cells) + 6 * s * double(n_cells);
+  }
+};
+
+// ------------------------------------------------------------------ DG ----
+template <typename T>
+class DGOperator final : public Operator {
+ public:
+  DevBuf<T> d_geo;      // [6 + 4 + (mass?1:0)][n_cells]
+  DevBuf<int32_t> d_nb; // [4][n_cells]
+  DevBuf<int8_t> d_nbf; // [4][n_cells]
+  DevBuf<T> d_Q;        // [n_cells][4][NC][NFQ] published face normal derivatives
+  bool has_mass = false;
+
+  DGOperator(const Mesh& mesh, const OpConfig& c) {
+    cfg = c;
+    const int p = cfg.degree;
+    K = k_of(p);
+    n_cells = mesh.n_cells;
+    m = int64_t(K) * cfg.n_components * n_cells;
+    n_interior_faces = mesh.n_interior_faces;
+    n_boundary_faces = mesh.n_boundary_faces;
+    has_mass = cfg.kind == FEM_HELMHOLTZ;
+    constrained.assign(m, 0);
+    support.resize(3 * size_t(K) * n_cells);
+    for (int64_t cc = 0; cc < n_cells; ++cc) {
+      const int32_t* cv = &mesh.cell_vertices[4 * cc];
+      for (int i = 0; i < K; ++i)
+        for (int a = 0; a < 3; ++a) {
+          double sum = 0;
+          for (int v = 0; v < 4; ++v) {
+            const int lat = p == 1 ? ref::Tables<1>::LATTICE[i][v]
+                                   : p == 2 ? ref::Tables<2>::LATTICE[i][v] : ref::Tables<3>::LATTICE[i][v];
+            sum += lat * mesh.x[3 * size_t(cv[v]) + a];
+          }
+          support[3 * (size_t(K) * cc + i) + a] = sum / p;
+        }
+    }
+    const int n_geo = has_mass ? 11 : 10;
+    std::vector<T> geo(size_t(n_geo) * n_cells);
+    // per-cell quantities for the penalty
+    std::vector<double> tau(n_cells), inv_h(4 * size_t(n_cells)), area(4 * size_t(n_cells));
+    std::vector<double> absdet(n_cells);
+    for (int64_t cc = 0; cc < n_cells; ++cc) {
+      const CellGeometry g = cell_geometry(mesh, cc);
+      absdet[cc] = std::fabs(g.det);
+      double G[6];
+      metric(g, G);
+      for (int k = 0; k < 6; ++k) geo[size_t(k) * n_cells + cc] = T(G[k]);
+      if (has_mass) geo[size_t(10) * n_cells + cc] = T(cfg.mass * absdet[cc]);
+      double surf = 0;
+      for (int f = 0; f < 4; ++f) {
+        double a, nrm[3];
+        face_area_normal(mesh, cc, f, a, nrm);
+        area[4 * cc + f] = a;
+        inv_h[4 * cc + f] = 2.0 * a / absdet[cc];  // |grad lambda_f| = 1/h_f
+        surf += a * (mesh.nb[4 * cc + f] < 0 ? 1.0 : 0.5);
+      }
+      tau[cc] = surf / (absdet[cc] / 6.0);
+    }
+    const double factor = cfg.penalty == FEM_PENALTY_SQUARE ? double((p + 1) * (p + 1))
+                                                            : double((p + 1) * (p + 3)) / 3.0;
+    for (int64_t cc = 0; cc < n_cells; ++cc)
+      for (int f = 0; f < 4; ++f) {
+        const int32_t nbc = mesh.nb[4 * cc + f];
+        double sigma;
+        if (cfg.kind == FEM_HELMHOLTZ) {
+          // 1/h normal to the face, averaged over both sides
+          // (application_helmholtz.cc:1329-1333 and :857-859 on the boundary)
+          sigma = nbc >= 0 ? factor * 0.5 * (inv_h[4 * cc + f] + inv_h[4 * size_t(nbc) + mesh.nbf[4 * cc + f]])
+                           : factor * inv_h[4 * cc + f];
+        } else {
+          // max of the two cells' surface/volume (DG/cells_batched/application.cc:1377-1379)
+          sigma = nbc >= 0 ? factor * std::max(tau[cc], tau[nbc]) : factor * tau[cc];
+        }
+        geo[size_t(6 + f) * n_cells + cc] = T(sigma * area[4 * cc + f]);
+      }
+    d_geo.upload(geo);
+    std::vector<int32_t> nb(4 * size_t(n_cells));
+    std::vector<int8_t> nbf(4 * size_t(n_cells));
+    for (int64_t cc = 0; cc < n_cells; ++cc)
+      for (int f = 0; f < 4; ++f) {
+        nb[size_t(f) * n_cells + cc] = mesh.nb[4 * cc + f];
+        nbf[size_t(f) * n_cells + cc] = mesh.nbf[4 * cc + f] < 0 ? 0 : mesh.nbf[4 * cc + f];
+      }
+    d_nb.upload(nb);
+    d_nbf.upload(nbf);
+    d_Q.alloc(size_t(n_cells) * 4 * cfg.n_components * nfq_of(p));
+  }
+
+  DGProblem<T> problem(const void* src, void* dst) const {
+    DGProblem<T> pr;
+    pr.geo = d_geo.p;
+    pr.nb = d_nb.p;
+    pr.nbf = d_nbf.p;
+    pr.src = static_cast<const T*>(src);
+    pr.dst = static_cast<T*>(dst);
+    pr.Q = d_Q.p;
+    pr.n_cells = n_cells;
+    return pr;
+  }
+
+  void vmult(void* dst, const void* src, cudaStream_t s) override {
+    DGBatch<T> b;
+    b.n = 1;
+    b.begin[0] = 0;
+    b.begin[1] = n_cells;
+    b.p[0] = problem(src, dst);
+    launch_dg(cfg, b, n_cells, s, 0);
+  }
+
+  void vmult_phase(void* dst, const void* src, int phase, cudaStream_t s) override {
+    DGBatch<T> b;
+    b.n = 1;
+    b.begin[0] = 0;
+    b.begin[1] = n_cells;
+    b.p[0] = problem(src, dst);
+    launch_dg(cfg, b, n_cells, s, phase);
+  }
+
+  void diagonal(void* diag, cudaStream_t s) override {
+    DGBatch<T> b;
+    b.n = 1;
+    b.begin[0] = 0;
+    b.begin[1] = n_cells;
+    b.p[0] = problem(nullptr, diag);
+    launch_dg(cfg, b, n_cells, s, 3);
+  }
+
+  void work(double& flops, double& bytes) const override {
+    const int p = cfg.degree, kq = kq_of(p), nf = nf_of(p), nfq = nfq_of(p), nz = nnz_grad_rt(p);
+    const double trace = 2.0 * (nz + 12 * nfq);
+    double apply = 2.0 * (2 * nz + 9 * kq + 3 * kq * kq) +
+                   4 * 2.0 * (3 * nfq + nf + nf * nf + nf + 2 * nf * nfq + 3 * nfq + 3 * nfq);
+    if (has_mass) apply += 2.0 * (K * K + K);
+    flops = (trace + apply) * cfg.n_components * double(n_cells);
+    const double s = double(sizeof(T));
+    bytes = 2 * s * double(m) + 6 * s * double(n_cells) + double(n_interior_faces) * (8 + s) +
+            double(n_boundary_faces) * (4 + s);
+  }
+
+  // Dispatch over a batch.  what: 0 trace+apply, 1 trace, 2 apply, 3 diagonal.
+  static void launch_dg(const OpConfig& cfg, const DGBatch<T>& b, int64_t n_total, cudaStream_t s, int what) {
+    const bool mass = cfg.kind == FEM_HELMHOLTZ;
+    const int nc = cfg.n_components;
+    SFEM_REQUIRE(nc == 1 || nc == 3, FEM_ERR_ARG, "DG: n_components must be 1 or 3");
+#define SFEM_DG_CASE(P, NC, MASS)                                                       \
+  if (cfg.degree == P && nc == NC && mass == MASS) {                                    \
+    run<P, NC, MASS>(b, n_total, s, what);                                              \
+    return;                                                                             \
+  }
+    SFEM_DG_CASE(1, 1, false) SFEM_DG_CASE(2, 1, false) SFEM_DG_CASE(3, 1, false)
+    SFEM_DG_CASE(1, 1, true) SFEM_DG_CASE(2, 1, true) SFEM_DG_CASE(3, 1, true)
+    SFEM_DG_CASE(1, 3, true) SFEM_DG_CASE(2, 3, true) SFEM_DG_CASE(3, 3, true)
+    SFEM_DG_CASE(1, 3, false) SFEM_DG_CASE(2, 3, false) SFEM_DG_CASE(3, 3, false)
+#undef SFEM_DG_CASE
+    throw Error(FEM_ERR_ARG, "DG: unsupported degree/components combination");
+  }
+
+  template <int P, int NC, bool MASS>
+  static void run(const DGBatch<T>& b, int64_t n_total, cudaStream_t s, int what) {
+    const unsigned grid = blocks_for(n_total, 128);
+    if (what == 3) {
+      dg_diagonal_kernel<P, NC, MASS, T><<<grid, 128, 0, s>>>(b, n_total);
+    } else {
+      if (what != 2) dg_trace_kernel<P, NC, T><<<grid, 128, 0, s>>>(b, n_total);
+      if (what != 1) dg_apply_kernel<P, NC, MASS, T><<<grid, 128, 0, s>>>(b, n_total);
+    }
+    SFEM_CUDA(cudaGetLastError());
+  }
+};
+
+template <typename T>
+class DGBatchImpl final : public Batch {
+ public:
+  std::vector<DGOperator<T>*> ops;
+  OpConfig cfg;
+  explicit DGBatchImpl(const std::vector<Operator*>& o) {
+    SFEM_REQUIRE(!o.empty() && int(o.size()) <= kMaxBatch, FEM_ERR_ARG, "batch: 1..40 operators");
+    cfg = o[0]->cfg;
+    for (auto* op : o) {
+      auto* d = dynamic_cast<DGOperator<T>*>(op);
+      SFEM_REQUIRE(d != nullptr, FEM_ERR_ARG, "batch: only DG/Helmholtz operators of one precision");
+      SFEM_REQUIRE(d->cfg.degree == cfg.degree && d->cfg.kind == cfg.kind &&
+                       d->cfg.n_components == cfg.n_components,
+                   FEM_ERR_ARG, "batch: operators must share kind, degree and components");
+      ops.push_back(d);
+    }
+  }
+  void vmult(void* const* dst, const void* const* src, cudaStream_t s) override {
+    DGBatch<T> b;
+    b.n = int32_t(ops.size());
+    b.begin[0] = 0;
+    for (size_t i = 0; i < ops.size(); ++i) {
+      b.p[i] = ops[i]->problem(src[i], dst[i]);
+      b.begin[i + 1] = b.begin[i] + ops[i]->n_cells;
+    }
+    DGOperator<T>::launch_dg(cfg, b, b.begin[ops.size()], s, 0);
+  }
+};
+
+}  // namespace
+
+void Operator::inverse_diagonal(void* diag, cudaStream_t s) {
+  diagonal(diag, s);
+  const unsigned grid = blocks_for(m, 256);
+  if (cfg.precision == FEM_FP64)
+    inverse_diagonal_kernel<double><<<grid, 256, 0, s>>>(m, static_cast<double*>(diag));
+  else
+    inverse_diagonal_kernel<float><<<grid, 256, 0, s>>>(m, static_cast<float*>(diag));
+  SFEM_CUDA(cudaGetLastError());
+}
+
+std::unique_ptr<Operator> make_operator(const Mesh& mesh, const OpConfig& cfg) {
+  SFEM_REQUIRE(cfg.degree >= 1 && cfg.degree <= 3, FEM_ERR_ARG, "operator: degree must be 1, 2 or 3");
+  SFEM_REQUIRE(cfg.precision == FEM_FP64 || cfg.precision == FEM_FP32, FEM_ERR_ARG, "operator: bad precision");
+  if (cfg.kind == FEM_CG) {
+    SFEM_REQUIRE(cfg.n_components == 1, FEM_ERR_ARG, "CG: n_components must be 1");
+    if (cfg.precision == FEM_FP64) return std::make_unique<CGOperator<double>>(mesh, cfg);
+    return std::make_unique<CGOperator<float>>(mesh, cfg);
+  }
+  if (cfg.kind == FEM_DG || cfg.kind == FEM_HELMHOLTZ) {
+    if (cfg.precision == FEM_FP64) return std::make_unique<DGOperator<double>>(mesh, cfg);
+    return std::make_unique<DGOperator<float>>(mesh, cfg);
+  }
+  throw Error(FEM_ERR_ARG, "operator: unknown kind");
+}
+
+std::unique_ptr<Batch> make_batch(const std::vector<Operator*>& ops) {
+  SFEM_REQUIRE(!ops.empty(), FEM_ERR_ARG, "batch: empty");
+  if (ops[0]->cfg.precision == FEM_FP64) return std::make_unique<DGBatchImpl<double>>(ops);
+  return std::make_unique<DGBatchImpl<float>>(ops);
+}
+
+}  // namespace sfem

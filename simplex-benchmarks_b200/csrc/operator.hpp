@@ -1,0 +1,99 @@
+// Matrix-free operators on the GPU: the object behind fem_op.
+#pragma once
+#include <cuda_runtime.h>
+
+#include <cstdint>
+#include <memory>
+#include <vector>
+
+#include "../../include/simplex_fem.h"
+#include "common.hpp"
+#include "mesh.hpp"
+
+namespace sfem {
+
+// Owning device buffer.
+template <class T>
+struct DevBuf {
+  T* p = nullptr;
+  size_t n = 0;
+  DevBuf() = default;
+  explicit DevBuf(size_t count) { alloc(count); }
+  DevBuf(const DevBuf&) = delete;
+  DevBuf& operator=(const DevBuf&) = delete;
+  DevBuf(DevBuf&& o) noexcept : p(o.p), n(o.n) { o.p = nullptr; o.n = 0; }
+  DevBuf& operator=(DevBuf&& o) noexcept {
+    if (this != &o) { release(); p = o.p; n = o.n; o.p = nullptr; o.n = 0; }
+    return *this;
+  }
+  ~DevBuf() { release(); }
+  void alloc(size_t count) {
+    release();
+    n = count;
+    if (count) {
+      cudaError_t e = cudaMalloc(&p, count * sizeof(T));
+      if (e != cudaSuccess) {
+        p = nullptr;
+        n = 0;
+        throw Error(FEM_ERR_CUDA, std::string("cudaMalloc: ") + cudaGetErrorString(e));
+      }
+    }
+  }
+  void upload(const T* host, size_t count) {
+    if (count != n) alloc(count);
+    if (count) {
+      cudaError_t e = cudaMemcpy(p, host, count * sizeof(T), cudaMemcpyHostToDevice);
+      if (e != cudaSuccess) throw Error(FEM_ERR_CUDA, std::string("cudaMemcpy: ") + cudaGetErrorString(e));
+    }
+  }
+  void upload(const std::vector<T>& v) { upload(v.data(), v.size()); }
+  void release() {
+    if (p) cudaFree(p);
+    p = nullptr;
+    n = 0;
+  }
+};
+
+struct OpConfig {
+  int degree = 2;
+  int kind = FEM_CG;
+  int precision = FEM_FP64;
+  double mass = 0.0;
+  int n_components = 1;
+  int penalty = FEM_PENALTY_REFERENCE;
+};
+
+class Operator {
+ public:
+  virtual ~Operator() = default;
+  OpConfig cfg;
+  int K = 0;               // DoFs per cell and component
+  int64_t n_cells = 0;
+  int64_t m = 0;           // vector length
+  int64_t n_interior_faces = 0, n_boundary_faces = 0;
+  std::vector<int32_t> cell_dofs;    // host copy of the dof map (CG)
+  std::vector<uint8_t> constrained;  // host mask [m]
+  std::vector<double> support;       // host support points [m/NC][3]
+
+  size_t elem_size() const { return cfg.precision == FEM_FP64 ? 8 : 4; }
+  virtual void vmult(void* dst, const void* src, cudaStream_t s) = 0;
+  // phase 1 / phase 2 of vmult (see fem_op_vmult_phase)
+  virtual void vmult_phase(void* dst, const void* src, int phase, cudaStream_t s) = 0;
+  virtual void diagonal(void* diag, cudaStream_t s) = 0;
+  void inverse_diagonal(void* diag, cudaStream_t s);
+  // flops of the fused kernels and algorithmic bytes (src+dst once, index and
+  // geometry data once) of one vmult
+  virtual void work(double& flops, double& bytes) const = 0;
+};
+
+std::unique_ptr<Operator> make_operator(const Mesh& mesh, const OpConfig& cfg);
+
+// Batched multi-problem DG launch.
+class Batch {
+ public:
+  virtual ~Batch() = default;
+  virtual void vmult(void* const* dst, const void* const* src, cudaStream_t s) = 0;
+};
+std::unique_ptr<Batch> make_batch(const std::vector<Operator*>& ops);
+
+}  // namespace sfem

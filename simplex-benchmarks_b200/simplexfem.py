@@ -1,0 +1,270 @@
+"""Python mirror of the deal.II-shaped operator interface over the C ABI.
+
+The classes here keep the names and argument meaning of the reference's
+Operator / MultigridPreconditioner interface (CG/cells_batched/application.cc:
+1040-1582, CG/cells_batched/application_ph.cc:1754-2023): ``vmult(dst, src)``,
+``Tvmult``, ``m()``, ``initialize_dof_vector``, ``compute_inverse_diagonal``.
+Vectors are CUDA tensors (torch is used only for device memory and streams);
+every call goes through ``libsimplexfem.so`` (include/simplex_fem.h).  There is
+no CPU fallback: a missing library raises at import of the first handle.
+"""
+import ctypes as C
+import os
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "libsimplexfem.so")
+
+FEM_OK = 0
+FEM_CG, FEM_DG, FEM_HELMHOLTZ = 0, 1, 2
+FEM_FP64, FEM_FP32 = 0, 1
+FEM_PENALTY_REFERENCE, FEM_PENALTY_SQUARE = 0, 1
+KINDS = {"cg": FEM_CG, "dg": FEM_DG, "helmholtz": FEM_HELMHOLTZ}
+PRECISIONS = {"fp64": FEM_FP64, "fp32": FEM_FP32}
+
+
+class FemError(RuntimeError):
+    def __init__(self, code, msg):
+        super().__init__(f"simplexfem error {code}: {msg}")
+        self.code = code
+
+
+class MeshDesc(C.Structure):
+    _fields_ = [("n", C.c_int32 * 3), ("lo", C.c_double * 3), ("hi", C.c_double * 3),
+                ("jitter", C.c_double), ("seed", C.c_uint64)]
+
+
+class OpParams(C.Structure):
+    _fields_ = [("mass_coefficient", C.c_double), ("n_components", C.c_int32),
+                ("penalty", C.c_int32), ("reserved", C.c_int32 * 6)]
+
+
+_lib = None
+
+# (name, restype, argtypes) of every exported entry point
+_PROTOS = [
+    ("fem_last_error_string", C.c_char_p, []),
+    ("fem_version", C.c_int, [C.POINTER(C.c_int32), C.POINTER(C.c_int32)]),
+    ("fem_mesh_create", C.c_int, [C.POINTER(MeshDesc), C.POINTER(C.c_void_p)]),
+    ("fem_mesh_destroy", C.c_int, [C.c_void_p]),
+    ("fem_mesh_sizes", C.c_int, [C.c_void_p] + [C.POINTER(C.c_int64)] * 4),
+    ("fem_mesh_copy_vertices", C.c_int, [C.c_void_p, C.c_void_p]),
+    ("fem_mesh_copy_cells", C.c_int, [C.c_void_p, C.c_void_p]),
+    ("fem_mesh_copy_neighbors", C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p]),
+    ("fem_mesh_cg_dofs", C.c_int, [C.c_void_p, C.c_int32, C.POINTER(C.c_int64), C.c_void_p, C.c_void_p]),
+    ("fem_op_create", C.c_int, [C.c_void_p, C.c_int32, C.c_int32, C.c_int32, C.POINTER(OpParams),
+                                C.POINTER(C.c_void_p)]),
+    ("fem_op_destroy", C.c_int, [C.c_void_p]),
+    ("fem_op_m", C.c_int, [C.c_void_p, C.POINTER(C.c_uint64)]),
+    ("fem_op_info", C.c_int, [C.c_void_p, C.POINTER(C.c_int32), C.POINTER(C.c_int32), C.POINTER(C.c_int32),
+                              C.POINTER(C.c_int32), C.POINTER(C.c_int64), C.POINTER(C.c_int32)]),
+    ("fem_op_copy_dof_map", C.c_int, [C.c_void_p, C.c_void_p]),
+    ("fem_op_copy_constrained", C.c_int, [C.c_void_p, C.c_void_p]),
+    ("fem_op_copy_support_points", C.c_int, [C.c_void_p, C.c_void_p]),
+    ("fem_op_vmult", C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]),
+    ("fem_op_vmult_phase", C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_int32, C.c_void_p]),
+    ("fem_op_Tvmult", C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]),
+    ("fem_op_compute_inverse_diagonal", C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p]),
+    ("fem_op_compute_diagonal", C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p]),
+    ("fem_op_work", C.c_int, [C.c_void_p, C.POINTER(C.c_double), C.POINTER(C.c_double)]),
+    ("fem_batch_create", C.c_int, [C.c_void_p, C.c_int32, C.POINTER(C.c_void_p)]),
+    ("fem_batch_destroy", C.c_int, [C.c_void_p]),
+    ("fem_batch_vmult", C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]),
+]
+
+
+def lib():
+    """Load libsimplexfem.so (raises if it has not been built)."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise FemError(-1, f"{LIB_PATH} is missing: run `make -C simplex-benchmarks_b200`")
+        L = C.CDLL(LIB_PATH)
+        for name, res, args in _PROTOS:
+            if hasattr(L, name):
+                fn = getattr(L, name)
+                fn.restype = res
+                fn.argtypes = args
+        _lib = L
+    return _lib
+
+
+def check(status):
+    if status != FEM_OK:
+        raise FemError(status, lib().fem_last_error_string().decode())
+
+
+def _stream_ptr(stream=None):
+    import torch
+    s = stream if stream is not None else torch.cuda.current_stream()
+    return C.c_void_p(s.cuda_stream)
+
+
+def _ptr(t):
+    return C.c_void_p(t.data_ptr())
+
+
+class Mesh:
+    """Kuhn-subdivided box (fem_mesh_create)."""
+
+    def __init__(self, n, lo=(0.0, 0.0, 0.0), hi=(1.0, 1.0, 1.0), jitter=0.0, seed=0):
+        if isinstance(n, int):
+            n = (n, n, n)
+        d = MeshDesc()
+        d.n[:] = list(n)
+        d.lo[:] = list(lo)
+        d.hi[:] = list(hi)
+        d.jitter = jitter
+        d.seed = seed
+        h = C.c_void_p()
+        check(lib().fem_mesh_create(C.byref(d), C.byref(h)))
+        self.handle = h
+        self.n, self.lo, self.hi, self.jitter, self.seed = tuple(n), tuple(lo), tuple(hi), jitter, seed
+        nv, nc, fi, fb = (C.c_int64() for _ in range(4))
+        check(lib().fem_mesh_sizes(h, C.byref(nv), C.byref(nc), C.byref(fi), C.byref(fb)))
+        self.n_vertices, self.n_cells = nv.value, nc.value
+        self.n_interior_faces, self.n_boundary_faces = fi.value, fb.value
+
+    def vertices(self):
+        a = np.empty((self.n_vertices, 3), np.float64)
+        check(lib().fem_mesh_copy_vertices(self.handle, a.ctypes.data))
+        return a
+
+    def cells(self):
+        a = np.empty((self.n_cells, 4), np.int32)
+        check(lib().fem_mesh_copy_cells(self.handle, a.ctypes.data))
+        return a
+
+    def neighbors(self):
+        nb = np.empty((self.n_cells, 4), np.int32)
+        nbf = np.empty((self.n_cells, 4), np.int8)
+        check(lib().fem_mesh_copy_neighbors(self.handle, nb.ctypes.data, nbf.ctypes.data))
+        return nb, nbf
+
+    def cg_dofs(self, degree):
+        n = C.c_int64()
+        check(lib().fem_mesh_cg_dofs(self.handle, degree, C.byref(n), None, None))
+        k = (degree + 1) * (degree + 2) * (degree + 3) // 6
+        cd = np.empty((self.n_cells, k), np.int32)
+        cm = np.empty(n.value, np.uint8)
+        check(lib().fem_mesh_cg_dofs(self.handle, degree, C.byref(n), cd.ctypes.data, cm.ctypes.data))
+        return cd, cm
+
+    def __del__(self):
+        if getattr(self, "handle", None) and _lib is not None:
+            _lib.fem_mesh_destroy(self.handle)
+            self.handle = None
+
+
+class Operator:
+    """Matrix-free operator (fem_op); the drop-in for the reference's Operator."""
+
+    def __init__(self, mesh, degree, kind="cg", precision="fp64", mass=1e5, n_components=None,
+                 penalty=FEM_PENALTY_REFERENCE):
+        self.mesh = mesh
+        k = KINDS[kind] if isinstance(kind, str) else kind
+        pr = PRECISIONS[precision] if isinstance(precision, str) else precision
+        p = OpParams()
+        p.mass_coefficient = mass
+        p.n_components = n_components or (3 if k == FEM_HELMHOLTZ else 1)
+        p.penalty = penalty
+        h = C.c_void_p()
+        check(lib().fem_op_create(mesh.handle, degree, k, pr, C.byref(p), C.byref(h)))
+        self.handle = h
+        self.kind, self.precision, self.degree = k, pr, degree
+        m = C.c_uint64()
+        check(lib().fem_op_m(h, C.byref(m)))
+        self._m = m.value
+        dpc, nc, ncomp = C.c_int32(), C.c_int64(), C.c_int32()
+        check(lib().fem_op_info(h, None, None, None, C.byref(dpc), C.byref(nc), C.byref(ncomp)))
+        self.dofs_per_cell, self.n_cells, self.n_components = dpc.value, nc.value, ncomp.value
+
+    @property
+    def dtype(self):
+        import torch
+        return torch.float64 if self.precision == FEM_FP64 else torch.float32
+
+    def m(self):
+        return self._m
+
+    def initialize_dof_vector(self):
+        import torch
+        return torch.zeros(self._m, dtype=self.dtype, device="cuda")
+
+    def _check_vec(self, v):
+        if not v.is_cuda or v.dtype != self.dtype or v.numel() != self._m or not v.is_contiguous():
+            raise FemError(1, f"vector must be a contiguous CUDA {self.dtype} tensor of length {self._m}")
+
+    def vmult(self, dst, src, stream=None):
+        self._check_vec(dst)
+        self._check_vec(src)
+        check(lib().fem_op_vmult(self.handle, _ptr(dst), _ptr(src), _stream_ptr(stream)))
+
+    def vmult_phase(self, dst, src, phase, stream=None):
+        self._check_vec(dst)
+        self._check_vec(src)
+        check(lib().fem_op_vmult_phase(self.handle, _ptr(dst), _ptr(src), phase, _stream_ptr(stream)))
+
+    def Tvmult(self, dst, src, stream=None):
+        self._check_vec(dst)
+        self._check_vec(src)
+        check(lib().fem_op_Tvmult(self.handle, _ptr(dst), _ptr(src), _stream_ptr(stream)))
+
+    def compute_inverse_diagonal(self, vec, stream=None):
+        self._check_vec(vec)
+        check(lib().fem_op_compute_inverse_diagonal(self.handle, _ptr(vec), _stream_ptr(stream)))
+
+    def compute_diagonal(self, vec, stream=None):
+        self._check_vec(vec)
+        check(lib().fem_op_compute_diagonal(self.handle, _ptr(vec), _stream_ptr(stream)))
+
+    def dof_map(self):
+        a = np.empty((self.n_cells, self.dofs_per_cell * self.n_components), np.int32)
+        check(lib().fem_op_copy_dof_map(self.handle, a.ctypes.data))
+        return a
+
+    def constrained(self):
+        a = np.empty(self._m, np.uint8)
+        check(lib().fem_op_copy_constrained(self.handle, a.ctypes.data))
+        return a
+
+    def support_points(self):
+        a = np.empty((self._m // self.n_components, 3), np.float64)
+        check(lib().fem_op_copy_support_points(self.handle, a.ctypes.data))
+        return a
+
+    def work(self):
+        f, b = C.c_double(), C.c_double()
+        check(lib().fem_op_work(self.handle, C.byref(f), C.byref(b)))
+        return f.value, b.value
+
+    def __del__(self):
+        if getattr(self, "handle", None) and _lib is not None:
+            _lib.fem_op_destroy(self.handle)
+            self.handle = None
+
+
+class Batch:
+    """Several independent DG/Helmholtz operators applied in one launch per phase."""
+
+    def __init__(self, ops):
+        self.ops = list(ops)
+        arr = (C.c_void_p * len(ops))(*[o.handle.value for o in ops])
+        h = C.c_void_p()
+        check(lib().fem_batch_create(arr, len(ops), C.byref(h)))
+        self.handle = h
+
+    def vmult(self, dsts, srcs, stream=None):
+        n = len(self.ops)
+        for o, d, s in zip(self.ops, dsts, srcs):
+            o._check_vec(d)
+            o._check_vec(s)
+        da = (C.c_void_p * n)(*[d.data_ptr() for d in dsts])
+        sa = (C.c_void_p * n)(*[s.data_ptr() for s in srcs])
+        check(lib().fem_batch_vmult(self.handle, da, sa, _stream_ptr(stream)))
+
+    def __del__(self):
+        if getattr(self, "handle", None) and _lib is not None:
+            _lib.fem_batch_destroy(self.handle)
+            self.handle = None

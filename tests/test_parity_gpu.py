@@ -1,0 +1,154 @@
+"""GPU vmult parity against the CPU oracle, through the C ABI.
+
+Tolerances: relative l2 <= 1e-12 for FP64 (the bar of the reference's own
+"optimized vs generic" check, CG/cells_batched/application.cc:1937-1940, which
+prints a difference that "should be 0"), <= 2e-6 for FP32 operators compared
+with the FP64 oracle on the same (rounded) input.
+"""
+import numpy as np
+import pytest
+
+import oracle as orc
+import simplexfem as sf
+from util import dg_interpolate, rel_l2, seeded_src
+
+pytestmark = pytest.mark.gpu
+
+KIND = {"cg": orc.CG, "dg": orc.DG, "helmholtz": orc.HELMHOLTZ}
+TOL = {"fp64": 1e-12, "fp32": 2e-6}
+
+
+def run_product(op, x):
+    import torch
+    src = torch.tensor(x, dtype=op.dtype, device="cuda")
+    dst = op.initialize_dof_vector()
+    op.vmult(dst, src)
+    torch.cuda.synchronize()
+    return dst.double().cpu().numpy()
+
+
+def oracle_input(op, x):
+    """The FP64 value of the input the product actually sees."""
+    return x.astype(np.float32).astype(np.float64) if op.precision == sf.FEM_FP32 else x
+
+
+@pytest.mark.parametrize("precision", ["fp64", "fp32"])
+@pytest.mark.parametrize("kind", ["cg", "dg", "helmholtz"])
+@pytest.mark.parametrize("p", [1, 2, 3])
+def test_vmult_parity_small(cuda, p, kind, precision):
+    mesh = sf.Mesh((5, 4, 3), jitter=0.1, seed=0)
+    op = sf.Operator(mesh, p, kind, precision)
+    o = orc.for_mesh(mesh, p, KIND[kind], n_components=op.n_components)
+    assert o.n == op.m()
+    x = seeded_src(op.m(), 1)
+    y = run_product(op, x)
+    ref = o.vmult(oracle_input(op, x))
+    assert rel_l2(y, ref) <= TOL[precision]
+
+
+def test_config1_cg_p2_full_size(cuda):
+    """16^3 x 6 tets, CG P2, jitter 0.1 (seed 0), src U[-1,1] (seed 1), FP64."""
+    mesh = sf.Mesh(16, jitter=0.1, seed=0)
+    op = sf.Operator(mesh, 2, "cg", "fp64")
+    assert op.m() == 35937
+    x = seeded_src(op.m(), 1)
+    y = run_product(op, x)
+    ref = orc.for_mesh(mesh, 2, orc.CG).vmult(x)
+    assert rel_l2(y, ref) <= 1e-12
+
+
+@pytest.mark.parametrize("precision", ["fp64", "fp32"])
+def test_config2_dg_p3_full_size(cuda, precision):
+    """32^3 x 6 tets, DG P3 SIPG, 3,932,160 DoFs, FP64 and FP32 vs the FP64 oracle."""
+    mesh = sf.Mesh(32, jitter=0.1, seed=0)
+    op = sf.Operator(mesh, 3, "dg", precision)
+    assert op.m() == 3932160
+    x = seeded_src(op.m(), 1)
+    y = run_product(op, x)
+    ref = orc.for_mesh(mesh, 3, orc.DG).vmult(oracle_input(op, x))
+    assert rel_l2(y, ref) <= TOL[precision]
+
+
+@pytest.mark.parametrize("kind", ["cg", "dg", "helmholtz"])
+@pytest.mark.parametrize("p", [1, 2, 3])
+def test_diagonal_parity(cuda, p, kind):
+    import torch
+    mesh = sf.Mesh(3, jitter=0.1, seed=2)
+    op = sf.Operator(mesh, p, kind, "fp64")
+    d = op.initialize_dof_vector()
+    op.compute_diagonal(d)
+    ref = orc.for_mesh(mesh, p, KIND[kind], n_components=op.n_components).diagonal()
+    assert rel_l2(d.cpu().numpy(), ref) <= 1e-12
+    inv = op.initialize_dof_vector()
+    op.compute_inverse_diagonal(inv)
+    r = np.where(np.abs(ref) > 1e-10, 1.0 / ref, 1.0)
+    assert rel_l2(inv.cpu().numpy(), r) <= 1e-12
+    torch.cuda.synchronize()
+
+
+def test_cg_constrained_rows_are_identity(cuda):
+    mesh = sf.Mesh(4, jitter=0.1, seed=0)
+    op = sf.Operator(mesh, 2, "cg")
+    x = seeded_src(op.m(), 7)
+    y = run_product(op, x)
+    c = op.constrained().astype(bool)
+    assert c.sum() > 0 and np.array_equal(y[c], x[c])
+
+
+def test_dg_deterministic(cuda):
+    mesh = sf.Mesh(6, jitter=0.1, seed=0)
+    op = sf.Operator(mesh, 3, "dg")
+    x = seeded_src(op.m(), 3)
+    assert np.array_equal(run_product(op, x), run_product(op, x))
+
+
+def test_repeated_vmults_stable(cuda):
+    """100 back-to-back vmults (the reference's timing loop) give the same result."""
+    import torch
+    mesh = sf.Mesh(8, jitter=0.1, seed=0)
+    op = sf.Operator(mesh, 3, "dg")
+    src = torch.tensor(seeded_src(op.m(), 1), device="cuda")
+    dst = op.initialize_dof_vector()
+    op.vmult(dst, src)
+    first = dst.clone()
+    for _ in range(100):
+        op.vmult(dst, src)
+    torch.cuda.synchronize()
+    assert torch.equal(first, dst)
+
+
+def test_dg_linear_consistency_full_size(cuda):
+    """Size-independent property at 32^3: interior cells annihilate linears."""
+    import torch
+    mesh = sf.Mesh(32, jitter=0.1, seed=0)
+    op = sf.Operator(mesh, 3, "dg")
+    u = dg_interpolate(mesh, 3, lambda X: 1.0 + 2 * X[:, 0] - 3 * X[:, 1] + 0.5 * X[:, 2])
+    y = run_product(op, u).reshape(mesh.n_cells, -1)
+    nb, _ = mesh.neighbors()
+    inner = np.all(nb >= 0, axis=1)
+    assert np.abs(y[inner]).max() < 1e-11 * np.abs(y).max()
+    torch.cuda.synchronize()
+
+
+@pytest.mark.parametrize("precision", ["fp64", "fp32"])
+def test_batch_matches_single(cuda, precision):
+    """Uneven Helmholtz problems in one launch equal their individual vmults."""
+    import torch
+    ops, srcs = [], []
+    for i, n in enumerate([2, 3, 5, 4]):
+        mesh = sf.Mesh(n, jitter=0.1, seed=i)
+        op = sf.Operator(mesh, 2, "helmholtz", precision)
+        ops.append(op)
+        srcs.append(torch.tensor(seeded_src(op.m(), 100 + i), dtype=op.dtype, device="cuda"))
+    b = sf.Batch(ops)
+    outs = [o.initialize_dof_vector() for o in ops]
+    b.vmult(outs, srcs)
+    for o, s, d in zip(ops, srcs, outs):
+        ref = o.initialize_dof_vector()
+        o.vmult(ref, s)
+        torch.cuda.synchronize()
+        assert torch.equal(ref, d)
+    # and one of them against the oracle
+    o0 = orc.for_mesh(ops[2].mesh, 2, orc.HELMHOLTZ, n_components=3)
+    x = srcs[2].double().cpu().numpy()
+    assert rel_l2(outs[2].double().cpu().numpy(), o0.vmult(x)) <= TOL[precision]
