@@ -127,6 +127,18 @@ int fem_op_copy_support_points(const fem_op* op, double* xyz /* [m/n_components]
  * (CG/cells_batched/application.cc:1167-1176, DG/cells_batched/application.cc:1319-1332,
  * application_helmholtz.cc:567-580): dst = A src.  dst and src must not alias. */
 int fem_op_vmult(fem_op* op, void* dst, const void* src, void* stream);
+/* Same product as fem_op_vmult for FEM_DG / FEM_HELMHOLTZ operators, for
+ * callers that must not allocate device memory at the call (their memory
+ * pool owns the device, or cudaMalloc's implicit synchronisation and
+ * unbounded latency are not allowed there).  No counterpart in the
+ * reference.  The call allocates nothing: its scratch is a 16 MiB static
+ * device array inside this library (held on every GPU that loads it until
+ * exit); operators needing more scratch are rejected with FEM_ERR_ARG (DG P3
+ * FP64: up to 87,381 cells).  All calls share that array, so calls that
+ * overlap on the GPU race; order them on one stream.  The first call on a
+ * device looks up the array's device address; make it before any stream
+ * capture. */
+int fem_op_vmult_static_scratch(fem_op* op, void* dst, const void* src, void* stream);
 /* Operator::Tvmult (CG/cells_batched/application.cc:1193-1197): the operator is symmetric. */
 int fem_op_Tvmult(fem_op* op, void* dst, const void* src, void* stream);
 /* Operator::compute_inverse_diagonal (CG/cells_batched/application_ph.cc:1382-1404):

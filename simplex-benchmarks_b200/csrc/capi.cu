@@ -6,18 +6,7 @@
 
 #include "../../include/simplex_fem.h"
 #include "common.hpp"
-#include "mesh.hpp"
-#include "operator.hpp"
-
-struct fem_mesh {
-  sfem::Mesh mesh;
-};
-struct fem_op {
-  std::unique_ptr<sfem::Operator> op;
-};
-struct fem_batch {
-  std::unique_ptr<sfem::Batch> batch;
-};
+#include "handles.hpp"
 
 namespace sfem {
 namespace {
@@ -28,23 +17,8 @@ const char* last_error() { return g_last_error.c_str(); }
 }  // namespace sfem
 
 namespace {
-template <class F>
-int guarded(F&& f) {
-  try {
-    f();
-    return FEM_OK;
-  } catch (const sfem::Error& e) {
-    sfem::set_last_error(e.what());
-    return e.code;
-  } catch (const std::bad_alloc&) {
-    sfem::set_last_error("host allocation failed");
-    return FEM_ERR_INTERNAL;
-  } catch (const std::exception& e) {
-    sfem::set_last_error(e.what());
-    return FEM_ERR_INTERNAL;
-  }
-}
-#define REQUIRE_PTR(p) SFEM_REQUIRE((p) != nullptr, FEM_ERR_ARG, #p " is NULL")
+using sfem::guarded;
+#define REQUIRE_PTR(p) SFEM_REQUIRE_PTR(p)
 }  // namespace
 
 extern "C" {

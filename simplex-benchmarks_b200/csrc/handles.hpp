@@ -1,0 +1,38 @@
+// Definitions of the opaque C ABI handles (shared by the extern "C" files).
+#pragma once
+#include <memory>
+
+#include "mesh.hpp"
+#include "operator.hpp"
+
+struct fem_mesh {
+  sfem::Mesh mesh;
+};
+struct fem_op {
+  std::unique_ptr<sfem::Operator> op;
+};
+struct fem_batch {
+  std::unique_ptr<sfem::Batch> batch;
+};
+
+namespace sfem {
+// Runs f, converting exceptions into a status code and the last-error string.
+template <class F>
+int guarded(F&& f) {
+  try {
+    f();
+    return FEM_OK;
+  } catch (const Error& e) {
+    set_last_error(e.what());
+    return e.code;
+  } catch (const std::bad_alloc&) {
+    set_last_error("host allocation failed");
+    return FEM_ERR_INTERNAL;
+  } catch (const std::exception& e) {
+    set_last_error(e.what());
+    return FEM_ERR_INTERNAL;
+  }
+}
+}  // namespace sfem
+
+#define SFEM_REQUIRE_PTR(p) SFEM_REQUIRE((p) != nullptr, FEM_ERR_ARG, #p " is NULL")

@@ -249,6 +249,19 @@ class DGOperator final : public Operator {
     launch_dg(cfg, b, n_cells, s, phase);
   }
 
+  size_t scratch_bytes() const override { return d_Q.n * sizeof(T); }
+
+  void vmult_with_scratch(void* dst, const void* src, void* scratch, size_t bytes, cudaStream_t s) override {
+    SFEM_REQUIRE(bytes >= scratch_bytes(), FEM_ERR_ARG, "vmult: scratch too small");
+    DGBatch<T> b;
+    b.n = 1;
+    b.begin[0] = 0;
+    b.begin[1] = n_cells;
+    b.p[0] = problem(src, dst);
+    b.p[0].Q = static_cast<T*>(scratch);
+    launch_dg(cfg, b, n_cells, s, 0);
+  }
+
   void diagonal(void* diag, cudaStream_t s) override {
     DGBatch<T> b;
     b.n = 1;

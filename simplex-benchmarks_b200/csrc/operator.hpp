@@ -80,6 +80,12 @@ class Operator {
   // phase 1 / phase 2 of vmult (see fem_op_vmult_phase)
   virtual void vmult_phase(void* dst, const void* src, int phase, cudaStream_t s) = 0;
   virtual void diagonal(void* diag, cudaStream_t s) = 0;
+  // Device scratch one vmult needs (DG: the published face traces; CG: none).
+  virtual size_t scratch_bytes() const { return 0; }
+  // vmult with the scratch supplied by the caller instead of the operator's own.
+  virtual void vmult_with_scratch(void* dst, const void* src, void* scratch, size_t bytes, cudaStream_t s) {
+    throw Error(FEM_ERR_ARG, "this operator kind uses no scratch memory");
+  }
   void inverse_diagonal(void* diag, cudaStream_t s);
   // flops of the fused kernels and algorithmic bytes (src+dst once, index and
   // geometry data once) of one vmult

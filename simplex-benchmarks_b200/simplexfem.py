@@ -64,6 +64,7 @@ _PROTOS = [
     ("fem_op_copy_support_points", C.c_int, [C.c_void_p, C.c_void_p]),
     ("fem_op_vmult", C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]),
     ("fem_op_vmult_phase", C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_int32, C.c_void_p]),
+    ("fem_op_vmult_static_scratch", C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]),
     ("fem_op_Tvmult", C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]),
     ("fem_op_compute_inverse_diagonal", C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p]),
     ("fem_op_compute_diagonal", C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p]),
