@@ -80,7 +80,9 @@ typedef struct fem_op_params {
   double mass_coefficient; /* FEM_HELMHOLTZ: factor of the mass term (reference: 1e5) */
   int32_t n_components;    /* FEM_HELMHOLTZ: number of fields (reference: 3); others: 1 */
   int32_t penalty;         /* FEM_DG: enum fem_penalty */
-  int32_t reserved[6];
+  int32_t kernel_variant;  /* 0: tuned default; DG/Helmholtz: 1 thread per cell x128 cells per
+                              CTA, 2 thread per cell x64, 3 warp roles x32 (autotuner knob) */
+  int32_t reserved[5];
 } fem_op_params;
 
 /* ---- library ----------------------------------------------------------- */
@@ -152,6 +154,10 @@ int fem_op_compute_diagonal(fem_op* op, void* diag, void* stream);
  * face normal derivatives and phase 2 runs the fused cell+face kernel.
  * Running phase 1 then phase 2 equals fem_op_vmult. */
 int fem_op_vmult_phase(fem_op* op, void* dst, const void* src, int32_t phase, void* stream);
+/* Switch the kernel form of an existing operator (same meaning as
+ * fem_op_params.kernel_variant); used by the autotuner.  No counterpart in
+ * the reference (deal.II picks its vectorisation at compile time). */
+int fem_op_set_kernel_variant(fem_op* op, int32_t variant);
 /* Algorithmic work of one vmult: flops and bytes of the fused kernels. */
 int fem_op_work(const fem_op* op, double* flops, double* bytes);
 

@@ -122,6 +122,8 @@ int fem_op_create(fem_mesh* mesh, int32_t degree, int32_t kind, int32_t precisio
         cfg.n_components = params->n_components > 0 ? params->n_components : 3;
       }
       cfg.penalty = params->penalty;
+      cfg.kernel_variant = params->kernel_variant;
+      SFEM_REQUIRE(cfg.kernel_variant >= 0 && cfg.kernel_variant <= 3, FEM_ERR_ARG, "kernel_variant must be 0..3");
       SFEM_REQUIRE(cfg.penalty == FEM_PENALTY_REFERENCE || cfg.penalty == FEM_PENALTY_SQUARE, FEM_ERR_ARG,
                    "penalty must be FEM_PENALTY_REFERENCE or FEM_PENALTY_SQUARE");
     }
@@ -225,6 +227,14 @@ int fem_op_compute_diagonal(fem_op* op, void* diag, void* stream) {
     REQUIRE_PTR(op);
     REQUIRE_PTR(diag);
     op->op->diagonal(diag, static_cast<cudaStream_t>(stream));
+  });
+}
+
+int fem_op_set_kernel_variant(fem_op* op, int32_t variant) {
+  return guarded([&] {
+    REQUIRE_PTR(op);
+    SFEM_REQUIRE(variant >= 0 && variant <= 3, FEM_ERR_ARG, "kernel_variant must be 0..3");
+    op->op->cfg.kernel_variant = variant;
   });
 }
 

@@ -430,6 +430,60 @@ def write_kernels(data, path):
         emit_matvec(L, d["MFPQ"], NFQ, NF, lambda r: f"o[{r}]", lambda c: f"j[{c}]", False, transpose=True)
         L.append("}")
         L.append("")
+    # single-row functions for warp-split kernels: a switch on the row index
+    # that folds away once the caller's loops are unrolled
+    for p, d in data.items():
+        K, KQ, NF, NFQ = d["K"], d["KQ"], d["NF"], d["NFQ"]
+
+        def row_switch(name, sig, rows, body_of_row):
+            L.append(f"template <typename T> __host__ __device__ __forceinline__ T {name}({sig}) {{")
+            L.append("  switch (r) {")
+            for r in range(rows):
+                L.append(f"    case {r}: return {body_of_row(r)};")
+            L.append("  }")
+            L.append("  return T(0);")
+            L.append("}")
+
+        def lin(coefs, term):
+            parts = []
+            for c, a in coefs:
+                if a == 0:
+                    continue
+                t = term(c)
+                if a == 1:
+                    parts.append(f"+ {t}")
+                elif a == -1:
+                    parts.append(f"- {t}")
+                else:
+                    parts.append(f"+ T({fmt(a)}) * {t}")
+            if not parts:
+                return "T(0)"
+            s = " ".join(parts)
+            return s[2:] if s.startswith("+ ") else "-" + s[2:] if False else ("T(0) " + s if s.startswith("-") else s[2:])
+
+        # grad row r = a*KQ + m from u[i*us]
+        row_switch(f"grad_row_P{p}", "int r, const T* u, int us", 3 * KQ,
+                   lambda r: lin([(i, d["D"][r // KQ][r % KQ][i]) for i in range(K)], lambda i: f"u[{i} * us]"))
+        # gradT row i from h[(a*KQ+m)*hs]
+        row_switch(f"gradT_row_P{p}", "int r, const T* h, int hs", K,
+                   lambda i: lin([(a * KQ + m, d["D"][a][m][i]) for a in range(3) for m in range(KQ)],
+                                 lambda c: f"h[{c} * hs]"))
+        # MQ row m from w[n]
+        row_switch(f"massQ_row_P{p}", "int r, const T* w", KQ,
+                   lambda m: lin([(n, d["MQ"][m][n]) for n in range(KQ)], lambda n: f"w[{n}]"))
+        # MP row i from u[j*us]
+        row_switch(f"massP_row_P{p}", "int r, const T* u, int us", K,
+                   lambda i: lin([(j, d["MP"][i][j]) for j in range(K)], lambda j: f"u[{j} * us]"))
+        # position of cell node i on face f (P_p) / of P_{p-1} node m on face f, -1 if absent
+        cases = " ".join(f"case {f*K+i}: return {d['FN'][f].index(i) if i in d['FN'][f] else -1};"
+                         for f in range(4) for i in range(K))
+        L.append(f"__host__ __device__ __forceinline__ constexpr int face_pos_P{p}(int f, int i) "
+                 f"{{ switch (f * {K} + i) {{ {cases} }} return -1; }}")
+        cases = " ".join(f"case {f*KQ+m}: return {d['FNQ'][f].index(m) if m in d['FNQ'][f] else -1};"
+                         for f in range(4) for m in range(KQ))
+        L.append(f"__host__ __device__ __forceinline__ constexpr int faceq_pos_P{p}(int f, int m) "
+                 f"{{ switch (f * {KQ} + m) {{ {cases} }} return -1; }}")
+        L.append("")
     # dispatch struct and runtime face-node tables
     for p, d in data.items():
         K, KQ, NF, NFQ = d["K"], d["KQ"], d["NF"], d["NFQ"]
@@ -450,6 +504,12 @@ def write_kernels(data, path):
         L.append(f"  template <class T> static __device__ __forceinline__ void facePQ(const T* a, T* o) {{ facePQ_P{p}(a, o); }}")
         L.append(f"  template <class T> static __device__ __forceinline__ void faceQP(const T* j, T* o) {{ faceQP_P{p}(j, o); }}")
         L.append(f"  static __device__ __forceinline__ int fn_runtime(int f, int i) {{ return cFN_P{p}[f][i]; }}")
+        L.append(f"  template <class T> static __device__ __forceinline__ T grad_row(int r, const T* u, int us) {{ return grad_row_P{p}(r, u, us); }}")
+        L.append(f"  template <class T> static __device__ __forceinline__ T gradT_row(int r, const T* h, int hs) {{ return gradT_row_P{p}(r, h, hs); }}")
+        L.append(f"  template <class T> static __device__ __forceinline__ T massQ_row(int r, const T* w) {{ return massQ_row_P{p}(r, w); }}")
+        L.append(f"  template <class T> static __device__ __forceinline__ T massP_row(int r, const T* u, int us) {{ return massP_row_P{p}(r, u, us); }}")
+        L.append(f"  static __host__ __device__ __forceinline__ constexpr int face_pos(int f, int i) {{ return face_pos_P{p}(f, i); }}")
+        L.append(f"  static __host__ __device__ __forceinline__ constexpr int faceq_pos(int f, int m) {{ return faceq_pos_P{p}(f, m); }}")
         cases = " ".join(f"case {f*NF+i}: return {d['FN'][f][i]};" for f in range(4) for i in range(NF))
         L.append(f"  static __host__ __device__ __forceinline__ constexpr int fn(int f, int i) {{ switch (f * {NF} + i) {{ {cases} }} return 0; }}")
         cases = " ".join(f"case {f*NFQ+i}: return {d['FNQ'][f][i]};" for f in range(4) for i in range(NFQ))

@@ -20,6 +20,13 @@
 // sorting every cell's vertices by global id removes the orientation part of
 // that bucket key, and the element-centric form removes the scatter.
 //
+// Memory: one thread per cell, BS cells per CTA.  A CTA's cells are
+// contiguous, so their DoF blocks (and their Q blocks) are one contiguous
+// range: it is copied into shared memory with coalesced loads, into rows
+// padded to an odd number of words (conflict-free per-thread reads), and the
+// results leave the same way.  Neighbours inside the CTA are read from shared
+// memory, the others from L2.
+//
 // Geometry per cell (structure of arrays, n_cells stride):
 //   [0..5]  G = |det J| J^-1 J^-T           (00,11,22,01,02,12)
 //   [6..9]  s_f = sigma_f |F_f|              (penalty times face area)
@@ -48,24 +55,40 @@ struct DGProblem {
   int64_t n_cells;
 };
 
-// Several independent problems in one launch; begin[] is the prefix sum of
-// their cell counts.  Passed by value as a kernel parameter.
+// Several independent problems in one launch.  Work is split in CTA-sized
+// blocks of cells that never straddle two problems; block_begin[] is the
+// prefix sum of the blocks per problem.  Passed as a __grid_constant__ kernel
+// parameter.
 template <typename T>
 struct DGBatch {
   int32_t n;
-  int64_t begin[kMaxBatch + 1];
+  int64_t block_begin[kMaxBatch + 1];
   DGProblem<T> p[kMaxBatch];
 };
 
 template <typename T>
-__device__ __forceinline__ int find_problem(const DGBatch<T>& b, int64_t gc) {
+__device__ __forceinline__ int find_problem(const DGBatch<T>& b, int64_t blk) {
   int lo = 0, hi = b.n - 1;
   while (lo < hi) {
     const int mid = (lo + hi + 1) >> 1;
-    if (b.begin[mid] <= gc) lo = mid; else hi = mid - 1;
+    if (b.block_begin[mid] <= blk) lo = mid; else hi = mid - 1;
   }
   return lo;
 }
+
+// row stride (in elements) of a staged per-cell block of n values: odd, so
+// that 32 threads reading their own rows hit 32 different banks
+__host__ __device__ constexpr int padded(int n) { return (n % 2) ? n : n + 1; }
+
+template <int P, int NC>
+struct DGShape {
+  using O = gen::Ops<P>;
+  static constexpr int K = O::K, KQ = O::KQ, NF = O::NF, NFQ = O::NFQ;
+  static constexpr int U = NC * K;           // values per cell
+  static constexpr int QN = 4 * NC * NFQ;    // published traces per cell
+  static constexpr int US = padded(U);       // staged row strides
+  static constexpr int QS = padded(QN);
+};
 
 // J^-1 (2|F_f| n_f) for local face f
 template <typename T>
@@ -83,83 +106,117 @@ __device__ __forceinline__ void face_cf(const T (&G)[6], int f, T (&cf)[3]) {
   }
 }
 
+// coalesced copy of `rows` rows of n contiguous values into padded rows
+template <int N, int S, int BS, typename T>
+__device__ __forceinline__ void stage_in(T* __restrict__ sm, const T* __restrict__ g, int rows) {
+  const int total = rows * N;
+  for (int e = threadIdx.x; e < total; e += BS) sm[(e / N) * S + (e % N)] = __ldg(g + e);
+}
+template <int N, int S, int BS, typename T>
+__device__ __forceinline__ void stage_out(T* __restrict__ g, const T* __restrict__ sm, int rows) {
+  const int total = rows * N;
+  for (int e = threadIdx.x; e < total; e += BS) g[e] = sm[(e / N) * S + (e % N)];
+}
+
 // Publish q_f = 2|F_f| d_n u (own outward normal) at the P_{p-1} nodes of every face.
-template <int P, int NC, typename T>
-__global__ void __launch_bounds__(128) dg_trace_kernel(const __grid_constant__ DGBatch<T> batch, int64_t n_total) {
+template <int P, int NC, int BS, typename T>
+__global__ void __launch_bounds__(BS) dg_trace_kernel(const __grid_constant__ DGBatch<T> batch, int64_t n_blocks) {
   using O = gen::Ops<P>;
-  for (int64_t gc = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; gc < n_total;
-       gc += int64_t(gridDim.x) * blockDim.x) {
-    const int pi = find_problem(batch, gc);
+  using S = DGShape<P, NC>;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  T* su = reinterpret_cast<T*>(smem_raw);  // [BS][US]
+  T* sq = su + BS * S::US;                 // [BS][QS]
+  for (int64_t blk = blockIdx.x; blk < n_blocks; blk += gridDim.x) {
+    const int pi = find_problem(batch, blk);
     const DGProblem<T>& pr = batch.p[pi];
-    const int64_t c = gc - batch.begin[pi];
-    const int64_t n = pr.n_cells;
-    T G[6];
+    const int64_t c0 = (blk - batch.block_begin[pi]) * BS;
+    const int nloc = int(pr.n_cells - c0 < BS ? pr.n_cells - c0 : int64_t(BS));
+    __syncthreads();
+    stage_in<S::U, S::US, BS>(su, pr.src + c0 * S::U, nloc);
+    __syncthreads();
+    const int t = threadIdx.x;
+    if (t < nloc) {
+      const int64_t c = c0 + t;
+      const int64_t n = pr.n_cells;
+      T G[6];
 #pragma unroll
-    for (int k = 0; k < 6; ++k) G[k] = __ldg(pr.geo + k * n + c);
+      for (int k = 0; k < 6; ++k) G[k] = __ldg(pr.geo + k * n + c);
 #pragma unroll
-    for (int comp = 0; comp < NC; ++comp) {
-      T u[O::K];
-      const T* s = pr.src + (c * NC + comp) * O::K;
+      for (int comp = 0; comp < NC; ++comp) {
+        T u[O::K];
 #pragma unroll
-      for (int i = 0; i < O::K; ++i) u[i] = __ldg(s + i);
-      T g[3 * O::KQ];
-      O::grad(u, g);
+        for (int i = 0; i < O::K; ++i) u[i] = su[t * S::US + comp * O::K + i];
+        T g[3 * O::KQ];
+        O::grad(u, g);
 #pragma unroll
-      for (int f = 0; f < 4; ++f) {
-        T cf[3];
-        face_cf(G, f, cf);
-        T* q = pr.Q + ((c * 4 + f) * NC + comp) * O::NFQ;
+        for (int f = 0; f < 4; ++f) {
+          T cf[3];
+          face_cf(G, f, cf);
 #pragma unroll
-        for (int m = 0; m < O::NFQ; ++m) {
-          const int nq = O::fnq(f, m);
-          q[m] = cf[0] * g[nq] + cf[1] * g[O::KQ + nq] + cf[2] * g[2 * O::KQ + nq];
+          for (int m = 0; m < O::NFQ; ++m) {
+            const int nq = O::fnq(f, m);
+            sq[t * S::QS + (f * NC + comp) * O::NFQ + m] =
+                cf[0] * g[nq] + cf[1] * g[O::KQ + nq] + cf[2] * g[2 * O::KQ + nq];
+          }
         }
       }
     }
+    __syncthreads();
+    stage_out<S::QN, S::QS, BS>(pr.Q + c0 * S::QN, sq, nloc);
   }
 }
 
-// Own-cell terms for one component; with HAVE_NB the neighbour traces come
-// from src/Q, otherwise (diagonal) they are zero.
+// Own-cell terms plus face terms for one component.  u and qm come from the
+// staged rows of this cell (`us`, `qs`); HAVE_NB reads the neighbour traces
+// (from shared memory when the neighbour is in this CTA, rows su/sq),
+// otherwise they are zero (diagonal).
 template <int P, int NC, bool MASS, bool HAVE_NB, typename T>
-__device__ __forceinline__ void dg_cell_component(const DGProblem<T>& pr, int64_t c, int comp,
+__device__ __forceinline__ void dg_cell_component(const DGProblem<T>& pr, int64_t c0, int comp,
+                                                  const T* us, const T* qs, const T* su, const T* sq, int nloc,
                                                   const T (&G)[6], const T (&sf)[4], T md,
                                                   const int32_t (&nb)[4], const int (&nbf)[4],
-                                                  const T (&u)[gen::Ops<P>::K], T (&y)[gen::Ops<P>::K]) {
+                                                  T (&y)[gen::Ops<P>::K]) {
   using O = gen::Ops<P>;
+  using S = DGShape<P, NC>;
   constexpr int K = O::K, KQ = O::KQ, NF = O::NF, NFQ = O::NFQ;
-  T g[3 * KQ];
-  O::grad(u, g);
+  const T* u = us + comp * K;
   T h[3 * KQ];
   {
+    T uu[K];
+#pragma unroll
+    for (int i = 0; i < K; ++i) uu[i] = u[i];
+    T g[3 * KQ];
+    O::grad(uu, g);
     T w[3 * KQ];
     apply_metric<KQ>(G, g, w);
 #pragma unroll
     for (int a = 0; a < 3; ++a) O::massQ(w + a * KQ, h + a * KQ);
-  }
 #pragma unroll
-  for (int i = 0; i < K; ++i) y[i] = T(0);
-  if (MASS) O::massP(u, md, y);
+    for (int i = 0; i < K; ++i) y[i] = T(0);
+    if (MASS) O::massP(uu, md, y);
+  }
 #pragma unroll
   for (int f = 0; f < 4; ++f) {
     T cf[3];
     face_cf(G, f, cf);
-    T qm[NFQ];
-#pragma unroll
-    for (int m = 0; m < NFQ; ++m) {
-      const int nq = O::fnq(f, m);
-      qm[m] = cf[0] * g[nq] + cf[1] * g[KQ + nq] + cf[2] * g[2 * KQ + nq];
-    }
+    const T* qm = qs + (f * NC + comp) * NFQ;
     T j[NF], avg[NFQ];
     if (nb[f] >= 0) {
-      // interior face: jump and average with the neighbour's published trace
       if (HAVE_NB) {
-        const T* us = pr.src + (int64_t(nb[f]) * NC + comp) * K;
-        const T* qs = pr.Q + ((int64_t(nb[f]) * 4 + nbf[f]) * NC + comp) * NFQ;
+        const int64_t lc = int64_t(nb[f]) - c0;
+        const T* un;
+        const T* qn;
+        if (lc >= 0 && lc < nloc) {
+          un = su + lc * S::US + comp * K;
+          qn = sq + lc * S::QS + (nbf[f] * NC + comp) * NFQ;
+        } else {
+          un = pr.src + (int64_t(nb[f]) * NC + comp) * K;
+          qn = pr.Q + ((int64_t(nb[f]) * 4 + nbf[f]) * NC + comp) * NFQ;
+        }
 #pragma unroll
-        for (int i = 0; i < NF; ++i) j[i] = u[O::fn(f, i)] - __ldg(us + O::fn_runtime(nbf[f], i));
+        for (int i = 0; i < NF; ++i) j[i] = u[O::fn(f, i)] - un[O::fn_runtime(nbf[f], i)];
 #pragma unroll
-        for (int m = 0; m < NFQ; ++m) avg[m] = T(0.25) * (qm[m] - __ldg(qs + m));
+        for (int m = 0; m < NFQ; ++m) avg[m] = T(0.25) * (qm[m] - qn[m]);
       } else {
 #pragma unroll
         for (int i = 0; i < NF; ++i) j[i] = u[O::fn(f, i)];
@@ -198,67 +255,106 @@ __device__ __forceinline__ void dg_cell_component(const DGProblem<T>& pr, int64_
   O::gradT(h, y);
 }
 
-template <int P, int NC, bool MASS, typename T>
-__global__ void __launch_bounds__(128) dg_apply_kernel(const __grid_constant__ DGBatch<T> batch, int64_t n_total) {
-  using O = gen::Ops<P>;
-  for (int64_t gc = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; gc < n_total;
-       gc += int64_t(gridDim.x) * blockDim.x) {
-    const int pi = find_problem(batch, gc);
-    const DGProblem<T>& pr = batch.p[pi];
-    const int64_t c = gc - batch.begin[pi];
-    const int64_t n = pr.n_cells;
-    T G[6], sf[4];
+template <typename T>
+struct CellData {
+  T G[6], sf[4], md;
+  int32_t nb[4];
+  int nbf[4];
+};
+
+template <bool MASS, typename T>
+__device__ __forceinline__ void load_cell(const DGProblem<T>& pr, int64_t c, CellData<T>& d) {
+  const int64_t n = pr.n_cells;
 #pragma unroll
-    for (int k = 0; k < 6; ++k) G[k] = __ldg(pr.geo + k * n + c);
+  for (int k = 0; k < 6; ++k) d.G[k] = __ldg(pr.geo + k * n + c);
 #pragma unroll
-    for (int f = 0; f < 4; ++f) sf[f] = __ldg(pr.geo + (6 + f) * n + c);
-    const T md = MASS ? __ldg(pr.geo + 10 * n + c) : T(0);
-    int32_t nb[4];
-    int nbf[4];
+  for (int f = 0; f < 4; ++f) d.sf[f] = __ldg(pr.geo + (6 + f) * n + c);
+  d.md = MASS ? __ldg(pr.geo + 10 * n + c) : T(0);
 #pragma unroll
-    for (int f = 0; f < 4; ++f) {
-      nb[f] = __ldg(pr.nb + f * n + c);
-      nbf[f] = __ldg(pr.nbf + f * n + c);
-    }
-#pragma unroll 1
-    for (int comp = 0; comp < NC; ++comp) {
-      T u[O::K], y[O::K];
-      const T* s = pr.src + (c * NC + comp) * O::K;
-#pragma unroll
-      for (int i = 0; i < O::K; ++i) u[i] = __ldg(s + i);
-      dg_cell_component<P, NC, MASS, true>(pr, c, comp, G, sf, md, nb, nbf, u, y);
-      T* d = pr.dst + (c * NC + comp) * O::K;
-#pragma unroll
-      for (int i = 0; i < O::K; ++i) d[i] = y[i];
-    }
+  for (int f = 0; f < 4; ++f) {
+    d.nb[f] = __ldg(pr.nb + f * n + c);
+    d.nbf[f] = __ldg(pr.nbf + f * n + c);
   }
 }
 
-// Diagonal of the DG operator: (A)_ii = own-cell terms applied to e_i.
-template <int P, int NC, bool MASS, typename T>
-__global__ void __launch_bounds__(128) dg_diagonal_kernel(const __grid_constant__ DGBatch<T> batch, int64_t n_total) {
+template <int P, int NC, bool MASS, int BS, typename T>
+__global__ void __launch_bounds__(BS, BS == 64 ? 6 : 1) dg_apply_kernel(const __grid_constant__ DGBatch<T> batch,
+                                                                       int64_t n_blocks) {
   using O = gen::Ops<P>;
-  for (int64_t gc = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; gc < n_total;
-       gc += int64_t(gridDim.x) * blockDim.x) {
-    const int pi = find_problem(batch, gc);
+  using S = DGShape<P, NC>;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  T* su = reinterpret_cast<T*>(smem_raw);  // [BS][US]  src rows
+  T* sq = su + BS * S::US;                 // [BS][QS]  published traces
+  T* sy = sq + BS * S::QS;                 // [BS][US]  results
+  for (int64_t blk = blockIdx.x; blk < n_blocks; blk += gridDim.x) {
+    const int pi = find_problem(batch, blk);
     const DGProblem<T>& pr = batch.p[pi];
-    const int64_t c = gc - batch.begin[pi];
-    const int64_t n = pr.n_cells;
-    T G[6], sf[4];
-    for (int k = 0; k < 6; ++k) G[k] = pr.geo[k * n + c];
-    for (int f = 0; f < 4; ++f) sf[f] = pr.geo[(6 + f) * n + c];
-    const T md = MASS ? pr.geo[10 * n + c] : T(0);
-    int32_t nb[4];
-    int nbf[4];
-    for (int f = 0; f < 4; ++f) {
-      nb[f] = pr.nb[f * n + c];
-      nbf[f] = pr.nbf[f * n + c];
-    }
-    for (int i = 0; i < O::K; ++i) {
-      T u[O::K], y[O::K];
+    const int64_t c0 = (blk - batch.block_begin[pi]) * BS;
+    const int nloc = int(pr.n_cells - c0 < BS ? pr.n_cells - c0 : int64_t(BS));
+    __syncthreads();
+    stage_in<S::U, S::US, BS>(su, pr.src + c0 * S::U, nloc);
+    stage_in<S::QN, S::QS, BS>(sq, pr.Q + c0 * S::QN, nloc);
+    __syncthreads();
+    const int t = threadIdx.x;
+    if (t < nloc) {
+      CellData<T> d;
+      load_cell<MASS>(pr, c0 + t, d);
+#pragma unroll 1
+      for (int comp = 0; comp < NC; ++comp) {
+        T y[O::K];
+        dg_cell_component<P, NC, MASS, true>(pr, c0, comp, su + t * S::US, sq + t * S::QS, su, sq, nloc, d.G,
+                                             d.sf, d.md, d.nb, d.nbf, y);
 #pragma unroll
-      for (int j = 0; j < O::K; ++j) u[j] = j == i ? T(1) : T(0);
-      dg_cell_component<P, NC, MASS, false>(pr, c, 0, G, sf, md, nb, nbf, u, y);
+        for (int i = 0; i < O::K; ++i) sy[t * S::US + comp * O::K + i] = y[i];
+      }
+    }
+    __syncthreads();
+    stage_out<S::U, S::US, BS>(pr.dst + c0 * S::U, sy, nloc);
+  }
+}
+
+// Diagonal of the DG operator: (A)_ii = own-cell terms applied to e_i, with
+// the own traces of e_i formed on the fly and the neighbour traces zero.
+// Set-up only: plain per-thread code, 128 cells per block of work.
+template <int P, int NC, bool MASS, typename T>
+__global__ void __launch_bounds__(128) dg_diagonal_kernel(const __grid_constant__ DGBatch<T> batch,
+                                                          int64_t n_blocks) {
+  using O = gen::Ops<P>;
+  using S1 = DGShape<P, 1>;
+  constexpr int BS = 128;
+  for (int64_t blk = blockIdx.x; blk < n_blocks; blk += gridDim.x) {
+    const int pi = find_problem(batch, blk);
+    const DGProblem<T>& pr = batch.p[pi];
+    const int64_t c = (blk - batch.block_begin[pi]) * BS + threadIdx.x;
+    if (c >= pr.n_cells) continue;
+    CellData<T> d;
+    load_cell<MASS>(pr, c, d);
+    for (int i = 0; i < O::K; ++i) {
+      T e[S1::US];
+      T q[S1::QS];
+#pragma unroll
+      for (int j = 0; j < O::K; ++j) e[j] = j == i ? T(1) : T(0);
+      {
+        T g[3 * O::KQ];
+        T uu[O::K];
+#pragma unroll
+        for (int j = 0; j < O::K; ++j) uu[j] = e[j];
+        O::grad(uu, g);
+#pragma unroll
+        for (int f = 0; f < 4; ++f) {
+          T cf[3];
+          face_cf(d.G, f, cf);
+#pragma unroll
+          for (int m = 0; m < O::NFQ; ++m) {
+            const int nq = O::fnq(f, m);
+            q[f * O::NFQ + m] = cf[0] * g[nq] + cf[1] * g[O::KQ + nq] + cf[2] * g[2 * O::KQ + nq];
+          }
+        }
+      }
+      T y[O::K];
+      // the diagonal is the same for every component
+      dg_cell_component<P, 1, MASS, false, T>(pr, 0, 0, e, q, nullptr, nullptr, 0, d.G, d.sf, d.md, d.nb, d.nbf,
+                                              y);
       T yi = T(0);
 #pragma unroll
       for (int j = 0; j < O::K; ++j)

@@ -5,6 +5,7 @@
 
 #include "kernels_cg.cuh"
 #include "kernels_dg.cuh"
+#include "kernels_dg3.cuh"
 #include "operator.hpp"
 #include "ref_tables.h"
 
@@ -232,43 +233,27 @@ class DGOperator final : public Operator {
   }
 
   void vmult(void* dst, const void* src, cudaStream_t s) override {
-    DGBatch<T> b;
-    b.n = 1;
-    b.begin[0] = 0;
-    b.begin[1] = n_cells;
-    b.p[0] = problem(src, dst);
-    launch_dg(cfg, b, n_cells, s, 0);
+    const DGProblem<T> pr = problem(src, dst);
+    launch_dg(cfg, &pr, 1, s, 0);
   }
 
   void vmult_phase(void* dst, const void* src, int phase, cudaStream_t s) override {
-    DGBatch<T> b;
-    b.n = 1;
-    b.begin[0] = 0;
-    b.begin[1] = n_cells;
-    b.p[0] = problem(src, dst);
-    launch_dg(cfg, b, n_cells, s, phase);
+    const DGProblem<T> pr = problem(src, dst);
+    launch_dg(cfg, &pr, 1, s, phase);
   }
 
   size_t scratch_bytes() const override { return d_Q.n * sizeof(T); }
 
   void vmult_with_scratch(void* dst, const void* src, void* scratch, size_t bytes, cudaStream_t s) override {
     SFEM_REQUIRE(bytes >= scratch_bytes(), FEM_ERR_ARG, "vmult: scratch too small");
-    DGBatch<T> b;
-    b.n = 1;
-    b.begin[0] = 0;
-    b.begin[1] = n_cells;
-    b.p[0] = problem(src, dst);
-    b.p[0].Q = static_cast<T*>(scratch);
-    launch_dg(cfg, b, n_cells, s, 0);
+    DGProblem<T> pr = problem(src, dst);
+    pr.Q = static_cast<T*>(scratch);
+    launch_dg(cfg, &pr, 1, s, 0);
   }
 
   void diagonal(void* diag, cudaStream_t s) override {
-    DGBatch<T> b;
-    b.n = 1;
-    b.begin[0] = 0;
-    b.begin[1] = n_cells;
-    b.p[0] = problem(nullptr, diag);
-    launch_dg(cfg, b, n_cells, s, 3);
+    const DGProblem<T> pr = problem(nullptr, diag);
+    launch_dg(cfg, &pr, 1, s, 3);
   }
 
   void work(double& flops, double& bytes) const override {
@@ -283,14 +268,16 @@ class DGOperator final : public Operator {
             double(n_boundary_faces) * (4 + s);
   }
 
-  // Dispatch over a batch.  what: 0 trace+apply, 1 trace, 2 apply, 3 diagonal.
-  static void launch_dg(const OpConfig& cfg, const DGBatch<T>& b, int64_t n_total, cudaStream_t s, int what) {
+  // Dispatch over n problems.  what: 0 trace+apply, 1 trace, 2 apply, 3 diagonal.
+  static void launch_dg(const OpConfig& cfg, const DGProblem<T>* probs, int n, cudaStream_t s, int what) {
     const bool mass = cfg.kind == FEM_HELMHOLTZ;
     const int nc = cfg.n_components;
     SFEM_REQUIRE(nc == 1 || nc == 3, FEM_ERR_ARG, "DG: n_components must be 1 or 3");
+    SFEM_REQUIRE(n >= 1 && n <= kMaxBatch, FEM_ERR_ARG, "DG: 1..40 problems per launch");
+    const int variant = cfg.kernel_variant > 0 ? cfg.kernel_variant : default_variant(cfg.degree, nc);
 #define SFEM_DG_CASE(P, NC, MASS)                                                       \
   if (cfg.degree == P && nc == NC && mass == MASS) {                                    \
-    run<P, NC, MASS>(b, n_total, s, what);                                              \
+    run<P, NC, MASS>(probs, n, s, what, variant);                                       \
     return;                                                                             \
   }
     SFEM_DG_CASE(1, 1, false) SFEM_DG_CASE(2, 1, false) SFEM_DG_CASE(3, 1, false)
@@ -301,14 +288,76 @@ class DGOperator final : public Operator {
     throw Error(FEM_ERR_ARG, "DG: unsupported degree/components combination");
   }
 
+  // kernel forms: 1 thread per cell, 128 cells per CTA; 2 thread per cell, 64
+  // cells per CTA; 3 warp roles, 32 cells per CTA
+  // (measured on B200: scalar P3 runs best register-capped at 64 cells per CTA,
+  // the 3-component forms at 128 cells per CTA)
+  static int default_variant(int p, int nc) { return (nc == 1 && p == 3) ? 2 : 1; }
+
+  static DGBatch<T> make_batch(const DGProblem<T>* probs, int n, int bs, int64_t& n_blocks) {
+    DGBatch<T> b;
+    b.n = n;
+    b.block_begin[0] = 0;
+    for (int i = 0; i < n; ++i) {
+      b.p[i] = probs[i];
+      b.block_begin[i + 1] = b.block_begin[i] + (probs[i].n_cells + bs - 1) / bs;
+    }
+    n_blocks = b.block_begin[n];
+    return b;
+  }
+
+  template <class K>
+  static void opt_in_smem(K kernel, size_t bytes, int& configured) {
+    int dev = 0;
+    SFEM_CUDA(cudaGetDevice(&dev));
+    if (!(configured & (1 << dev))) {
+      SFEM_CUDA(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, int(bytes)));
+      configured |= 1 << dev;
+    }
+  }
+
+  template <int P, int NC, bool MASS, int BS>
+  static void run_cell(const DGProblem<T>* probs, int n, cudaStream_t s, int what) {
+    using S = DGShape<P, NC>;
+    int64_t n_blocks = 0;
+    const DGBatch<T> b = make_batch(probs, n, BS, n_blocks);
+    const size_t sm_trace = size_t(BS) * (S::US + S::QS) * sizeof(T);
+    const size_t sm_apply = size_t(BS) * (2 * S::US + S::QS) * sizeof(T);
+    static int conf_t = 0, conf_a = 0;
+    opt_in_smem(dg_trace_kernel<P, NC, BS, T>, sm_trace, conf_t);
+    opt_in_smem(dg_apply_kernel<P, NC, MASS, BS, T>, sm_apply, conf_a);
+    if (what != 2) dg_trace_kernel<P, NC, BS, T><<<unsigned(n_blocks), BS, sm_trace, s>>>(b, n_blocks);
+    if (what != 1) dg_apply_kernel<P, NC, MASS, BS, T><<<unsigned(n_blocks), BS, sm_apply, s>>>(b, n_blocks);
+  }
+
   template <int P, int NC, bool MASS>
-  static void run(const DGBatch<T>& b, int64_t n_total, cudaStream_t s, int what) {
-    const unsigned grid = blocks_for(n_total, 128);
+  static void run_warp(const DGProblem<T>* probs, int n, cudaStream_t s, int what) {
+    using D = DG3<P, NC>;
+    int64_t n_blocks = 0;
+    const DGBatch<T> b = make_batch(probs, n, D::CELLS, n_blocks);
+    const size_t sm_trace = size_t(D::TRACE_ELEMS) * sizeof(T);
+    const size_t sm_apply = size_t(D::APPLY_ELEMS) * sizeof(T);
+    static int conf_t = 0, conf_a = 0;
+    opt_in_smem(dg3_trace_kernel<P, NC, T>, sm_trace, conf_t);
+    opt_in_smem(dg3_apply_kernel<P, NC, MASS, T>, sm_apply, conf_a);
+    if (what != 2) dg3_trace_kernel<P, NC, T><<<unsigned(n_blocks), D::THREADS, sm_trace, s>>>(b, n_blocks);
+    if (what != 1) dg3_apply_kernel<P, NC, MASS, T><<<unsigned(n_blocks), D::THREADS, sm_apply, s>>>(b, n_blocks);
+  }
+
+  template <int P, int NC, bool MASS>
+  static void run(const DGProblem<T>* probs, int n, cudaStream_t s, int what, int variant) {
     if (what == 3) {
-      dg_diagonal_kernel<P, NC, MASS, T><<<grid, 128, 0, s>>>(b, n_total);
+      int64_t n_blocks = 0;
+      const DGBatch<T> b = make_batch(probs, n, 128, n_blocks);
+      dg_diagonal_kernel<P, NC, MASS, T><<<unsigned(n_blocks), 128, 0, s>>>(b, n_blocks);
+    } else if (variant == 1) {
+      run_cell<P, NC, MASS, 128>(probs, n, s, what);
+    } else if (variant == 2) {
+      run_cell<P, NC, MASS, 64>(probs, n, s, what);
+    } else if (variant == 3) {
+      run_warp<P, NC, MASS>(probs, n, s, what);
     } else {
-      if (what != 2) dg_trace_kernel<P, NC, T><<<grid, 128, 0, s>>>(b, n_total);
-      if (what != 1) dg_apply_kernel<P, NC, MASS, T><<<grid, 128, 0, s>>>(b, n_total);
+      throw Error(FEM_ERR_ARG, "DG: kernel variant must be 0..3");
     }
     SFEM_CUDA(cudaGetLastError());
   }
@@ -332,14 +381,9 @@ class DGBatchImpl final : public Batch {
     }
   }
   void vmult(void* const* dst, const void* const* src, cudaStream_t s) override {
-    DGBatch<T> b;
-    b.n = int32_t(ops.size());
-    b.begin[0] = 0;
-    for (size_t i = 0; i < ops.size(); ++i) {
-      b.p[i] = ops[i]->problem(src[i], dst[i]);
-      b.begin[i + 1] = b.begin[i] + ops[i]->n_cells;
-    }
-    DGOperator<T>::launch_dg(cfg, b, b.begin[ops.size()], s, 0);
+    DGProblem<T> probs[kMaxBatch];
+    for (size_t i = 0; i < ops.size(); ++i) probs[i] = ops[i]->problem(src[i], dst[i]);
+    DGOperator<T>::launch_dg(cfg, probs, int(ops.size()), s, 0);
   }
 };
 

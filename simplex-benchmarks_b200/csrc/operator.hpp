@@ -61,6 +61,7 @@ struct OpConfig {
   double mass = 0.0;
   int n_components = 1;
   int penalty = FEM_PENALTY_REFERENCE;
+  int kernel_variant = 0;  // 0: tuned default (see fem_op_params.kernel_variant)
 };
 
 class Operator {

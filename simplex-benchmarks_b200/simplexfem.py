@@ -37,7 +37,7 @@ class MeshDesc(C.Structure):
 
 class OpParams(C.Structure):
     _fields_ = [("mass_coefficient", C.c_double), ("n_components", C.c_int32),
-                ("penalty", C.c_int32), ("reserved", C.c_int32 * 6)]
+                ("penalty", C.c_int32), ("kernel_variant", C.c_int32), ("reserved", C.c_int32 * 5)]
 
 
 _lib = None
@@ -68,6 +68,7 @@ _PROTOS = [
     ("fem_op_Tvmult", C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]),
     ("fem_op_compute_inverse_diagonal", C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p]),
     ("fem_op_compute_diagonal", C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p]),
+    ("fem_op_set_kernel_variant", C.c_int, [C.c_void_p, C.c_int32]),
     ("fem_op_work", C.c_int, [C.c_void_p, C.POINTER(C.c_double), C.POINTER(C.c_double)]),
     ("fem_batch_create", C.c_int, [C.c_void_p, C.c_int32, C.POINTER(C.c_void_p)]),
     ("fem_batch_destroy", C.c_int, [C.c_void_p]),
@@ -234,6 +235,9 @@ class Operator:
         a = np.empty((self._m // self.n_components, 3), np.float64)
         check(lib().fem_op_copy_support_points(self.handle, a.ctypes.data))
         return a
+
+    def set_kernel_variant(self, variant):
+        check(lib().fem_op_set_kernel_variant(self.handle, variant))
 
     def work(self):
         f, b = C.c_double(), C.c_double()
