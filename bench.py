@@ -43,6 +43,7 @@ def parse():
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-solve", action="store_true", help="skip the multigrid solve measurement")
     return ap.parse_args()
 
 
@@ -156,6 +157,40 @@ def build_problem(precision):
     op = sf.Operator(mesh, DEGREE, "dg", precision)
     x = np.random.default_rng(1).uniform(-1.0, 1.0, op.m())
     return mesh, op, x
+
+
+def mg_solve_bench(repeats=5):
+    """Poisson solve to rel. residual 1e-8: CG P3 on 64^3 x 6 tets (7,189,057 DoFs),
+    f = sum of 8 sin(k.x), k ~ U[1,6]^3 (PCG64 seed 2); FP64 outer CG preconditioned by
+    the hybrid p(3-2-1)/h(64-32-16-8-4) multigrid with Chebyshev(3)-Jacobi smoothing and a
+    CUDA-graph V-cycle; levels in FP32 (mixed) vs FP64."""
+    import torch
+    import simplexfem as sf
+    mesh = sf.Mesh(64)
+    op = sf.Operator(mesh, 3, "cg", "fp64")
+    b = sf.rhs(op, sf.sine_modes_rhs())
+    x = op.initialize_dof_vector()
+    out = {"workload": "CG P3 Poisson, 64^3 x 6 Kuhn tets, 7,189,057 DoFs, rel. residual 1e-8",
+           "dofs": op.m()}
+    for prec in ("fp64", "fp32"):
+        mg = sf.Multigrid(op, precision=prec, smoother_degree=3)
+        cg = sf.SolverCG(op, mg)
+        cg.solve(x, b, rtol=1e-8)  # warm-up (graph capture)
+        times, its = [], None
+        for _ in range(repeats):
+            x.zero_()
+            torch.cuda.synchronize()
+            t0 = time.perf_counter()
+            r = cg.solve(x, b, rtol=1e-8)
+            torch.cuda.synchronize()
+            times.append(time.perf_counter() - t0)
+            its = r["iterations"]
+            assert r["status"] == 0
+        key = "fp64_mg" if prec == "fp64" else "mixed_mg"
+        out[key] = {"ms": 1e3 * min(times), "ms_median": 1e3 * statistics.median(times), "iterations": its,
+                    "dofs_per_s": op.m() / min(times)}
+        del cg, mg
+    return out
 
 
 def cpu_baseline(mesh, x, target_seconds=12.0):
@@ -298,6 +333,7 @@ def run_ours(args):
     achieved_gbs = alg_bytes / (apply_ms / 1e3) / 1e9
     vm_ms = statistics.mean(t64)
     fp64_peak = fp64_peak_tflops() if rank == 0 else None
+    solve = mg_solve_bench() if (rank == 0 and not args.no_solve) else None
 
     if rank == 0:
         line = {
@@ -320,6 +356,7 @@ def run_ours(args):
             "kernels_ms": {"dg_trace_kernel": statistics.mean(t_trace), "dg_apply_kernel": apply_ms,
                            "vmult": vm_ms},
             "extra": {"fp32_value": value32, "fp32_ms_per_step": sum(t32) / args.steps},
+            "solve": solve,
             "clocks": clk.summary(),
             "gpu_launches": 2 * args.steps,
         }

@@ -161,6 +161,80 @@ int fem_op_set_kernel_variant(fem_op* op, int32_t variant);
 /* Algorithmic work of one vmult: flops and bytes of the fused kernels. */
 int fem_op_work(const fem_op* op, double* flops, double* bytes);
 
+/* ---- loads --------------------------------------------------------------
+ * f(x) = sum_m amp[m] sin(k[m] . x)           (kind FEM_RHS_PLANE_WAVES)
+ *      = sum_m amp[m] prod_d sin(k[m][d] x_d)  (kind FEM_RHS_SINE_PRODUCTS) */
+enum { FEM_RHS_PLANE_WAVES = 0, FEM_RHS_SINE_PRODUCTS = 1 };
+typedef struct fem_rhs_desc {
+  int32_t kind;
+  int32_t n_modes; /* <= 16 */
+  double k[16][3];
+  double amp[16];
+} fem_rhs_desc;
+/* Operator::rhs (CG/cells_batched/application_ph.cc:1361-1367,1435-1458):
+ * dst_i = (f, phi_i); 0 on constrained CG DoFs; every DG component gets f. */
+int fem_op_rhs(fem_op* op, const fem_rhs_desc* f, void* dst, void* stream);
+/* nodal interpolant of f (VectorTools::interpolate; reference error checks
+ * application_ph.cc:2210-2213) */
+int fem_op_interpolate(fem_op* op, const fem_rhs_desc* f, void* dst, void* stream);
+
+/* ---- hybrid multigrid ----------------------------------------------------
+ * MultigridPreconditioner (CG/cells_batched/application_ph.cc:1754-2023):
+ * levels P1 on the coarsest mesh .. P1 on the fine mesh, then P2 .. Pp
+ * (FEM_MG_PH, application_ph.cc) or P1 .. Pp on the coarsest mesh, then Pp on
+ * finer meshes (FEM_MG_HP, application_hp.cc:1819-1843); Chebyshev-Jacobi
+ * smoothing; dense FP64 coarse solve; optional CUDA-graph V-cycle.  The fine
+ * operator must be FEM_CG on a cubic mesh with n / coarse_n a power of two;
+ * the mesh must outlive the hierarchy. */
+enum { FEM_MG_PH = 0, FEM_MG_HP = 1 };
+typedef struct fem_mg_params {
+  int32_t order;            /* FEM_MG_PH / FEM_MG_HP */
+  int32_t precision;        /* level precision: FEM_FP32 (mixed) or FEM_FP64 */
+  int32_t smoother_degree;  /* Chebyshev degree (reference 5, benchmark 3) */
+  int32_t eig_iterations;   /* CG steps of the eigenvalue estimate (10) */
+  double smoothing_range;   /* lambda_max / lambda_min (20) */
+  double eig_safety;        /* lambda_max = safety * estimate (1.2) */
+  int32_t coarse_n;         /* hexes per direction on the coarsest level (4) */
+  int32_t use_graph;        /* capture the V-cycle as a CUDA graph (1) */
+  int32_t reserved[4];
+} fem_mg_params;
+int fem_mg_params_default(fem_mg_params* p);
+int fem_mg_create(fem_op* fine, const fem_mg_params* p, fem_mg** out);
+int fem_mg_destroy(fem_mg* mg);
+int fem_mg_n_levels(const fem_mg* mg, int32_t* n);
+int fem_mg_level_info(const fem_mg* mg, int32_t level, uint64_t* m, int32_t* degree, int32_t* hexes,
+                      double* lambda_max);
+/* PreconditionMG::vmult: dst = V(src), FP64 vectors of the fine operator */
+int fem_mg_vcycle(fem_mg* mg, double* dst, const double* src, void* stream);
+/* MG hooks on level-precision vectors of length level m: mg::Matrix::vmult,
+ * MGSmootherPrecondition::smooth, MGTwoLevelTransfer::prolongate_and_add /
+ * restrict_and_add (level -> level-1), MGCoarseGridBase::operator()
+ * (application_ph.cc:1714-1746) */
+int fem_mg_level_vmult(fem_mg* mg, int32_t level, void* dst, const void* src, void* stream);
+int fem_mg_smooth(fem_mg* mg, int32_t level, void* x, const void* b, int32_t zero_initial, void* stream);
+int fem_mg_prolongate_add(fem_mg* mg, int32_t level, void* dst, const void* src, void* stream);
+int fem_mg_restrict_add(fem_mg* mg, int32_t level, void* dst, const void* src, void* stream);
+int fem_mg_coarse_solve(fem_mg* mg, void* dst, const void* src, void* stream);
+
+/* ---- preconditioned CG ---------------------------------------------------
+ * SolverCG (application_ph.cc:1949-1980) on an FP64 operator; stops when
+ * ||r|| <= rtol ||b||.  status: FEM_OK, FEM_ERR_NOT_CONVERGED,
+ * FEM_ERR_BREAKDOWN (p^T A p <= 0) or FEM_ERR_NONFINITE. */
+enum { FEM_PRECOND_NONE = 0, FEM_PRECOND_JACOBI = 1, FEM_PRECOND_MG = 2 };
+typedef struct fem_solve_info {
+  int32_t iterations;
+  int32_t status;
+  double initial_residual;
+  double final_residual;
+} fem_solve_info;
+typedef struct fem_cg fem_cg;
+/* flexible != 0: Polak-Ribiere beta (flexible CG, for variable preconditioners) */
+int fem_cg_create(fem_op* op, fem_mg* mg /* FEM_PRECOND_MG only */, int32_t precond, int32_t flexible,
+                  fem_cg** out);
+int fem_cg_destroy(fem_cg* cg);
+int fem_cg_solve(fem_cg* cg, double* x, const double* b, double rtol, int32_t max_iterations,
+                 fem_solve_info* info, void* stream);
+
 /* ---- batched multi-problem launch (components-batched Helmholtz etc.) ----
  * All operators must share kind, degree, precision and n_components.  One
  * persistent launch per phase covers every problem. */

@@ -302,7 +302,7 @@ def build(pmax=3):
         data[p] = dict(K=K, KQ=KQ, NF=NF, NFQ=NFQ, D=D, MQ=MQ, MP=MP, FN=FN, FNQ=FNQ,
                        MFPP=MFPP, MFPQ=MFPQ, EMB=EMB,
                        NODES=[node_pos(a, p) for a in Bp.nodes],
-                       LATTICE=Bp.nodes)
+                       LATTICE=Bp.nodes, MONO=Bp.mono, COEF=Bp.coef)
     return data
 
 
@@ -340,6 +340,9 @@ def write_tables(data, path):
         if d["EMB"] is not None:
             kq = len(d["EMB"][0])
             out.append(arr("EMB", "double", d["EMB"], [d["K"], kq]))
+        # basis polynomials: phi_n(x,y,z) = sum_m COEF[n][m] x^MONO[m][0] y^MONO[m][1] z^MONO[m][2]
+        out.append(arr("MONO", "int", [list(m) for m in d["MONO"]], [len(d["MONO"]), 3]))
+        out.append(arr("COEF", "double", d["COEF"], [d["K"], len(d["MONO"])]))
         out.append("};\n\n")
     out.append("}  // namespace ref\n}  // namespace sfem\n")
     with open(path, "w") as fh:

@@ -3,6 +3,7 @@
 #include <memory>
 
 #include "mesh.hpp"
+#include "mg.hpp"
 #include "operator.hpp"
 
 struct fem_mesh {
@@ -13,6 +14,13 @@ struct fem_op {
 };
 struct fem_batch {
   std::unique_ptr<sfem::Batch> batch;
+};
+struct fem_mg {
+  std::unique_ptr<sfem::Multigrid> mg;
+};
+struct fem_cg {
+  std::unique_ptr<sfem::Preconditioner> own_precond;
+  std::unique_ptr<sfem::CGSolver> solver;
 };
 
 namespace sfem {

@@ -1,0 +1,97 @@
+// Hybrid (p/h) multigrid V-cycle and the preconditioned CG solver.
+//
+// Replaces MultigridPreconditioner (CG/cells_batched/application_ph.cc:
+// 1754-2023, h-then-p order application_hp.cc:1735-2008) and SolverCG +
+// PreconditionMG (application_ph.cc:1949-1980).
+#pragma once
+#include <cuda_runtime.h>
+
+#include <memory>
+#include <vector>
+
+#include "operator.hpp"
+
+namespace sfem {
+
+enum MGOrder { MG_ORDER_PH = 0, MG_ORDER_HP = 1 };
+
+struct MGParams {
+  int order = MG_ORDER_PH;      // p-coarsening first, then h (reference _ph); or h first (_hp)
+  int precision = FEM_FP32;     // level operators, smoothers and transfers
+  int smoother_degree = 3;      // Chebyshev degree (reference: 5)
+  double smoothing_range = 20;  // lambda_min = lambda_max / range
+  int eig_iterations = 10;      // CG steps of the eigenvalue estimate
+  double eig_safety = 1.2;      // lambda_max = safety * estimate
+  int coarse_n = 4;             // hexes per direction of the coarsest mesh
+  int use_graph = 1;            // capture the V-cycle in a CUDA graph
+};
+
+class Multigrid {
+ public:
+  virtual ~Multigrid() = default;
+  MGParams params;
+  virtual int n_levels() const = 0;
+  virtual int64_t level_m(int l) const = 0;
+  virtual int level_degree(int l) const = 0;
+  virtual int level_hexes(int l) const = 0;
+  virtual double level_lambda_max(int l) const = 0;
+  // dst = V(src), FP64 vectors of the fine operator
+  virtual void vcycle(double* dst, const double* src, cudaStream_t s) = 0;
+  // level hooks (level-precision vectors of length level_m)
+  virtual void level_vmult(int l, void* dst, const void* src, cudaStream_t s) = 0;
+  virtual void smooth(int l, void* x, const void* b, bool zero_initial, cudaStream_t s) = 0;
+  virtual void prolongate_add(int l, void* dst, const void* src, cudaStream_t s) = 0;  // l-1 -> l
+  virtual void restrict_add(int l, void* dst, const void* src, cudaStream_t s) = 0;    // l -> l-1
+  virtual void coarse_solve(void* dst, const void* src, cudaStream_t s) = 0;
+  virtual Operator& level_operator(int l) = 0;
+};
+
+std::unique_ptr<Multigrid> make_multigrid(const Operator& fine, const MGParams& p);
+
+struct SolveInfo {
+  int iterations = 0;
+  int status = 0;  // FEM_OK, FEM_ERR_NOT_CONVERGED, FEM_ERR_BREAKDOWN, FEM_ERR_NONFINITE
+  double r0 = 0, rn = 0;
+};
+
+// Preconditioner interface for the CG solver (FP64 vectors of the fine operator)
+class Preconditioner {
+ public:
+  virtual ~Preconditioner() = default;
+  virtual void apply(double* dst, const double* src, cudaStream_t s) = 0;
+};
+
+class CGSolver {
+ public:
+  // flexible: Polak-Ribiere beta (for preconditioners that change between applications)
+  CGSolver(Operator& A, Preconditioner* M, bool flexible);
+  SolveInfo solve(double* x, const double* b, double rtol, int maxit, cudaStream_t s);
+  double dot(const double* x, const double* y, cudaStream_t s);
+
+ private:
+  Operator& A_;
+  Preconditioner* M_;
+  bool flexible_;
+  DevBuf<double> r_, z_, p_, q_, zold_, partial_;
+  double* host_ = nullptr;
+};
+
+class MGPreconditioner final : public Preconditioner {
+ public:
+  explicit MGPreconditioner(Multigrid& mg) : mg_(mg) {}
+  void apply(double* dst, const double* src, cudaStream_t s) override { mg_.vcycle(dst, src, s); }
+
+ private:
+  Multigrid& mg_;
+};
+
+class JacobiPreconditioner final : public Preconditioner {
+ public:
+  explicit JacobiPreconditioner(Operator& A);
+  void apply(double* dst, const double* src, cudaStream_t s) override;
+
+ private:
+  DevBuf<double> inv_;
+};
+
+}  // namespace sfem

@@ -125,6 +125,8 @@ class CGOperator final : public Operator {
     SFEM_CUDA(cudaGetLastError());
   }
 
+  const int32_t* device_dof_table() const override { return d_dofs.p; }
+
   void work(double& flops, double& bytes) const override {
     const int p = cfg.degree, kq = kq_of(p);
     const double per_cell = 2.0 * (2 * nnz_grad_rt(p) + 9 * kq + 3 * kq * kq);
@@ -402,16 +404,19 @@ void Operator::inverse_diagonal(void* diag, cudaStream_t s) {
 std::unique_ptr<Operator> make_operator(const Mesh& mesh, const OpConfig& cfg) {
   SFEM_REQUIRE(cfg.degree >= 1 && cfg.degree <= 3, FEM_ERR_ARG, "operator: degree must be 1, 2 or 3");
   SFEM_REQUIRE(cfg.precision == FEM_FP64 || cfg.precision == FEM_FP32, FEM_ERR_ARG, "operator: bad precision");
+  std::unique_ptr<Operator> op;
   if (cfg.kind == FEM_CG) {
     SFEM_REQUIRE(cfg.n_components == 1, FEM_ERR_ARG, "CG: n_components must be 1");
-    if (cfg.precision == FEM_FP64) return std::make_unique<CGOperator<double>>(mesh, cfg);
-    return std::make_unique<CGOperator<float>>(mesh, cfg);
+    if (cfg.precision == FEM_FP64) op = std::make_unique<CGOperator<double>>(mesh, cfg);
+    else op = std::make_unique<CGOperator<float>>(mesh, cfg);
+  } else if (cfg.kind == FEM_DG || cfg.kind == FEM_HELMHOLTZ) {
+    if (cfg.precision == FEM_FP64) op = std::make_unique<DGOperator<double>>(mesh, cfg);
+    else op = std::make_unique<DGOperator<float>>(mesh, cfg);
+  } else {
+    throw Error(FEM_ERR_ARG, "operator: unknown kind");
   }
-  if (cfg.kind == FEM_DG || cfg.kind == FEM_HELMHOLTZ) {
-    if (cfg.precision == FEM_FP64) return std::make_unique<DGOperator<double>>(mesh, cfg);
-    return std::make_unique<DGOperator<float>>(mesh, cfg);
-  }
-  throw Error(FEM_ERR_ARG, "operator: unknown kind");
+  op->mesh = &mesh;
+  return op;
 }
 
 std::unique_ptr<Batch> make_batch(const std::vector<Operator*>& ops) {

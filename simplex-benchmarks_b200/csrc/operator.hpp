@@ -68,6 +68,7 @@ class Operator {
  public:
   virtual ~Operator() = default;
   OpConfig cfg;
+  const Mesh* mesh = nullptr;  // the mesh the operator was built on (must outlive it)
   int K = 0;               // DoFs per cell and component
   int64_t n_cells = 0;
   int64_t m = 0;           // vector length
@@ -81,6 +82,8 @@ class Operator {
   // phase 1 / phase 2 of vmult (see fem_op_vmult_phase)
   virtual void vmult_phase(void* dst, const void* src, int phase, cudaStream_t s) = 0;
   virtual void diagonal(void* diag, cudaStream_t s) = 0;
+  // CG: device table [K][n_cells] of global DoFs, -1 at constrained ones
+  virtual const int32_t* device_dof_table() const { return nullptr; }
   // Device scratch one vmult needs (DG: the published face traces; CG: none).
   virtual size_t scratch_bytes() const { return 0; }
   // vmult with the scratch supplied by the caller instead of the operator's own.
@@ -91,7 +94,19 @@ class Operator {
   // flops of the fused kernels and algorithmic bytes (src+dst once, index and
   // geometry data once) of one vmult
   virtual void work(double& flops, double& bytes) const = 0;
+  // dst = (f, v_i) for the load described by `rhs` (CG: 0 on constrained DoFs)
+  virtual void rhs(const struct RhsDesc& rhs, void* dst, cudaStream_t s);
 };
+
+// f(x) = sum_m amp[m] sin(k[m] . x)            (kind 0, sum of plane waves)
+//      = sum_m amp[m] prod_d sin(k[m][d] x_d)   (kind 1, products)
+struct RhsDesc {
+  int kind = 0;
+  int n_modes = 0;
+  double k[16][3] = {};
+  double amp[16] = {};
+};
+double rhs_value(const RhsDesc& r, const double* x);
 
 std::unique_ptr<Operator> make_operator(const Mesh& mesh, const OpConfig& cfg);
 

@@ -40,6 +40,27 @@ class OpParams(C.Structure):
                 ("penalty", C.c_int32), ("kernel_variant", C.c_int32), ("reserved", C.c_int32 * 5)]
 
 
+class RhsDesc(C.Structure):
+    _fields_ = [("kind", C.c_int32), ("n_modes", C.c_int32), ("k", (C.c_double * 3) * 16),
+                ("amp", C.c_double * 16)]
+
+
+class MGParams(C.Structure):
+    _fields_ = [("order", C.c_int32), ("precision", C.c_int32), ("smoother_degree", C.c_int32),
+                ("eig_iterations", C.c_int32), ("smoothing_range", C.c_double), ("eig_safety", C.c_double),
+                ("coarse_n", C.c_int32), ("use_graph", C.c_int32), ("reserved", C.c_int32 * 4)]
+
+
+class SolveInfo(C.Structure):
+    _fields_ = [("iterations", C.c_int32), ("status", C.c_int32), ("initial_residual", C.c_double),
+                ("final_residual", C.c_double)]
+
+
+FEM_RHS_PLANE_WAVES, FEM_RHS_SINE_PRODUCTS = 0, 1
+FEM_MG_PH, FEM_MG_HP = 0, 1
+FEM_PRECOND_NONE, FEM_PRECOND_JACOBI, FEM_PRECOND_MG = 0, 1, 2
+FEM_ERR_NOT_CONVERGED, FEM_ERR_BREAKDOWN, FEM_ERR_NONFINITE = 4, 5, 6
+
 _lib = None
 
 # (name, restype, argtypes) of every exported entry point
@@ -70,6 +91,24 @@ _PROTOS = [
     ("fem_op_compute_diagonal", C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p]),
     ("fem_op_set_kernel_variant", C.c_int, [C.c_void_p, C.c_int32]),
     ("fem_op_work", C.c_int, [C.c_void_p, C.POINTER(C.c_double), C.POINTER(C.c_double)]),
+    ("fem_op_rhs", C.c_int, [C.c_void_p, C.POINTER(RhsDesc), C.c_void_p, C.c_void_p]),
+    ("fem_op_interpolate", C.c_int, [C.c_void_p, C.POINTER(RhsDesc), C.c_void_p, C.c_void_p]),
+    ("fem_mg_params_default", C.c_int, [C.POINTER(MGParams)]),
+    ("fem_mg_create", C.c_int, [C.c_void_p, C.POINTER(MGParams), C.POINTER(C.c_void_p)]),
+    ("fem_mg_destroy", C.c_int, [C.c_void_p]),
+    ("fem_mg_n_levels", C.c_int, [C.c_void_p, C.POINTER(C.c_int32)]),
+    ("fem_mg_level_info", C.c_int, [C.c_void_p, C.c_int32, C.POINTER(C.c_uint64), C.POINTER(C.c_int32),
+                                    C.POINTER(C.c_int32), C.POINTER(C.c_double)]),
+    ("fem_mg_vcycle", C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]),
+    ("fem_mg_level_vmult", C.c_int, [C.c_void_p, C.c_int32, C.c_void_p, C.c_void_p, C.c_void_p]),
+    ("fem_mg_smooth", C.c_int, [C.c_void_p, C.c_int32, C.c_void_p, C.c_void_p, C.c_int32, C.c_void_p]),
+    ("fem_mg_prolongate_add", C.c_int, [C.c_void_p, C.c_int32, C.c_void_p, C.c_void_p, C.c_void_p]),
+    ("fem_mg_restrict_add", C.c_int, [C.c_void_p, C.c_int32, C.c_void_p, C.c_void_p, C.c_void_p]),
+    ("fem_mg_coarse_solve", C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]),
+    ("fem_cg_create", C.c_int, [C.c_void_p, C.c_void_p, C.c_int32, C.c_int32, C.POINTER(C.c_void_p)]),
+    ("fem_cg_destroy", C.c_int, [C.c_void_p]),
+    ("fem_cg_solve", C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_double, C.c_int32,
+                               C.POINTER(SolveInfo), C.c_void_p]),
     ("fem_batch_create", C.c_int, [C.c_void_p, C.c_int32, C.POINTER(C.c_void_p)]),
     ("fem_batch_destroy", C.c_int, [C.c_void_p]),
     ("fem_batch_vmult", C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]),
@@ -272,4 +311,125 @@ class Batch:
     def __del__(self):
         if getattr(self, "handle", None) and _lib is not None:
             _lib.fem_batch_destroy(self.handle)
+            self.handle = None
+
+
+def rhs_desc(modes, kind=FEM_RHS_PLANE_WAVES):
+    """modes: list of (k(3), amp)."""
+    d = RhsDesc()
+    d.kind = kind
+    d.n_modes = len(modes)
+    for m, (k, a) in enumerate(modes):
+        for j in range(3):
+            d.k[m][j] = float(k[j])
+        d.amp[m] = float(a)
+    return d
+
+
+def sine_modes_rhs(n_modes=8, seed=2, kmin=1.0, kmax=6.0):
+    """f = sum of n_modes sin(k.x), k uniform in [kmin, kmax]^3 from numpy PCG64(seed)."""
+    ks = np.random.default_rng(seed).uniform(kmin, kmax, (n_modes, 3))
+    return rhs_desc([(k, 1.0) for k in ks])
+
+
+def rhs(op, desc, dst=None, stream=None):
+    dst = op.initialize_dof_vector() if dst is None else dst
+    check(lib().fem_op_rhs(op.handle, C.byref(desc), _ptr(dst), _stream_ptr(stream)))
+    return dst
+
+
+def interpolate(op, desc, dst=None, stream=None):
+    dst = op.initialize_dof_vector() if dst is None else dst
+    check(lib().fem_op_interpolate(op.handle, C.byref(desc), _ptr(dst), _stream_ptr(stream)))
+    return dst
+
+
+class Multigrid:
+    """Hybrid p/h multigrid on a CG operator (fem_mg); MultigridPreconditioner's shape."""
+
+    def __init__(self, fine_op, order=FEM_MG_PH, precision="fp32", smoother_degree=3, smoothing_range=20.0,
+                 eig_iterations=10, eig_safety=1.2, coarse_n=4, use_graph=True):
+        p = MGParams()
+        check(lib().fem_mg_params_default(C.byref(p)))
+        p.order = order
+        p.precision = PRECISIONS[precision] if isinstance(precision, str) else precision
+        p.smoother_degree = smoother_degree
+        p.smoothing_range = smoothing_range
+        p.eig_iterations = eig_iterations
+        p.eig_safety = eig_safety
+        p.coarse_n = coarse_n
+        p.use_graph = int(bool(use_graph))
+        h = C.c_void_p()
+        check(lib().fem_mg_create(fine_op.handle, C.byref(p), C.byref(h)))
+        self.handle = h
+        self.fine = fine_op
+        self.precision = p.precision
+        n = C.c_int32()
+        check(lib().fem_mg_n_levels(h, C.byref(n)))
+        self.n_levels = n.value
+
+    def level_info(self, level):
+        m, d, hx, lm = C.c_uint64(), C.c_int32(), C.c_int32(), C.c_double()
+        check(lib().fem_mg_level_info(self.handle, level, C.byref(m), C.byref(d), C.byref(hx), C.byref(lm)))
+        return {"m": m.value, "degree": d.value, "hexes": hx.value, "lambda_max": lm.value}
+
+    def level_vector(self, level):
+        import torch
+        dt = torch.float64 if self.precision == FEM_FP64 else torch.float32
+        return torch.zeros(self.level_info(level)["m"], dtype=dt, device="cuda")
+
+    def vmult(self, dst, src, stream=None):
+        """PreconditionMG::vmult: dst = V(src) (FP64 fine vectors)."""
+        check(lib().fem_mg_vcycle(self.handle, _ptr(dst), _ptr(src), _stream_ptr(stream)))
+
+    def level_vmult(self, level, dst, src, stream=None):
+        check(lib().fem_mg_level_vmult(self.handle, level, _ptr(dst), _ptr(src), _stream_ptr(stream)))
+
+    def smooth(self, level, x, b, zero_initial=True, stream=None):
+        check(lib().fem_mg_smooth(self.handle, level, _ptr(x), _ptr(b), int(zero_initial), _stream_ptr(stream)))
+
+    def prolongate_add(self, level, dst, src, stream=None):
+        check(lib().fem_mg_prolongate_add(self.handle, level, _ptr(dst), _ptr(src), _stream_ptr(stream)))
+
+    def restrict_add(self, level, dst, src, stream=None):
+        check(lib().fem_mg_restrict_add(self.handle, level, _ptr(dst), _ptr(src), _stream_ptr(stream)))
+
+    def coarse_solve(self, dst, src, stream=None):
+        check(lib().fem_mg_coarse_solve(self.handle, _ptr(dst), _ptr(src), _stream_ptr(stream)))
+
+    def __del__(self):
+        if getattr(self, "handle", None) and _lib is not None:
+            _lib.fem_mg_destroy(self.handle)
+            self.handle = None
+
+
+class SolverCG:
+    """Preconditioned CG on an FP64 operator (fem_cg); SolverCG's shape."""
+
+    def __init__(self, op, preconditioner=None, flexible=False):
+        if isinstance(preconditioner, Multigrid):
+            kind, mgh = FEM_PRECOND_MG, preconditioner.handle
+        elif preconditioner == "jacobi":
+            kind, mgh = FEM_PRECOND_JACOBI, None
+        else:
+            kind, mgh = FEM_PRECOND_NONE, None
+        h = C.c_void_p()
+        check(lib().fem_cg_create(op.handle, mgh, kind, int(flexible), C.byref(h)))
+        self.handle = h
+        self.op = op
+        self.pre = preconditioner
+
+    def solve(self, x, b, rtol=1e-8, max_iterations=1000, stream=None, raise_on_failure=False):
+        info = SolveInfo()
+        rc = lib().fem_cg_solve(self.handle, _ptr(x), _ptr(b), rtol, max_iterations, C.byref(info),
+                                _stream_ptr(stream))
+        if rc not in (FEM_OK, FEM_ERR_NOT_CONVERGED, FEM_ERR_BREAKDOWN, FEM_ERR_NONFINITE) or (
+                raise_on_failure and rc != FEM_OK):
+            check(rc)
+        return {"iterations": info.iterations, "status": info.status, "r0": info.initial_residual,
+                "rn": info.final_residual}
+
+    def __del__(self):
+        if getattr(self, "handle", None) and _lib is not None:
+            _lib.fem_cg_destroy(self.handle)
             self.handle = None

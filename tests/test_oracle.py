@@ -118,3 +118,19 @@ def test_cg_diagonal_matches_unit_vectors():
         e = np.zeros(o.n)
         e[i] = 1
         assert abs(o.vmult(e)[i] - d[i]) < 1e-13 * max(1.0, abs(d[i]))
+
+
+@pytest.mark.parametrize("p,order", [(2, "ph"), (3, "hp")])
+def test_mg_oracle_converges_mesh_independently(p, order):
+    """The CPU multigrid oracle itself: few PCG iterations, independent of h."""
+    import mg_oracle as mgo
+    its = []
+    for n in (4, 8):
+        M = mgo.MGOracle(lambda k: sf.Mesh(k), n, p, order=order, coarse_n=2)
+        top = M.levels[-1]
+        b = np.random.default_rng(3).uniform(-1, 1, top.n)
+        b[top.cm.astype(bool)] = 0
+        x, it = mgo.pcg(lambda v: top.A @ v, b, M.vcycle, 1e-8, 100)
+        assert np.linalg.norm(b - top.A @ x) <= 1e-8 * np.linalg.norm(b)
+        its.append(it)
+    assert max(its) <= 12 and abs(its[0] - its[1]) <= 2, its
