@@ -226,6 +226,9 @@ typedef struct fem_solve_info {
   int32_t status;
   double initial_residual;
   double final_residual;
+  int32_t fallback_iteration; /* iteration at which a learned smoother was replaced by
+                                 Chebyshev (0: never) */
+  int32_t reserved;
 } fem_solve_info;
 typedef struct fem_cg fem_cg;
 /* flexible != 0: Polak-Ribiere beta (flexible CG, for variable preconditioners) */
@@ -234,6 +237,58 @@ int fem_cg_create(fem_op* op, fem_mg* mg /* FEM_PRECOND_MG only */, int32_t prec
 int fem_cg_destroy(fem_cg* cg);
 int fem_cg_solve(fem_cg* cg, double* x, const double* b, double rtol, int32_t max_iterations,
                  fem_solve_info* info, void* stream);
+
+/* ---- learned finest-level smoother ----------------------------------------
+ * No counterpart in the reference (its levels are always smoothed by
+ * PreconditionChebyshev).  A per-cell MLP 29 -> 64 -> 64 -> 20 (GELU, BF16
+ * weights, FP32 accumulation) maps a P3 cell's residual r_K / ||r_K|| and its
+ * Jacobian J_K / h_K to a correction scaled by ||r_K|| / h_K; corrections are
+ * assembled with inverse-multiplicity weights.  Trained on residual/error
+ * pairs of the multigrid-preconditioned CG on Kuhn meshes; used on the finest
+ * level of a P3 hierarchy inside flexible CG, with Chebyshev as fallback when
+ * one outer iteration reduces the residual by less than a factor 2. */
+typedef struct fem_mlp_train_params {
+  int32_t n_sizes;      /* number of data meshes (<= 4) */
+  int32_t sizes[4];     /* hexes per direction (16, 32) */
+  int32_t rhs_per_size; /* random sin-mode loads per mesh (seeds seed + 100 size + i) */
+  int32_t iterates;     /* MG-CG iterates per solve taken as samples */
+  int32_t samples;      /* total residual/error cell samples (200000) */
+  int32_t epochs;
+  int32_t batch;
+  float lr;             /* Adam learning rate */
+  double jitter;
+  uint64_t seed;
+  double noise_fraction;     /* share of samples from white-noise errors e with r = A e (0) */
+  int32_t coarse_iterations; /* V-cycle iterations of the coarse-grid correction removed from the
+                                solver's errors before they become targets (12) */
+  int32_t reserved;
+} fem_mlp_train_params;
+typedef struct fem_mlp_train_info {
+  int32_t samples;
+  int32_t reserved;
+  double loss_first; /* mean loss of the first epoch */
+  double loss_last;
+  double seconds;
+} fem_mlp_train_info;
+int fem_mlp_create(uint64_t seed, fem_mlp** out);
+int fem_mlp_destroy(fem_mlp* mlp);
+int fem_mlp_n_params(int32_t* n);
+int fem_mlp_get_weights(const fem_mlp* mlp, float* host /* [n_params] */);
+int fem_mlp_set_weights(fem_mlp* mlp, const float* host);
+int fem_mlp_train_params_default(fem_mlp_train_params* p);
+int fem_mlp_generate_and_train(fem_mlp* mlp, const fem_mlp_train_params* p, fem_mlp_train_info* info);
+/* training on device samples X [n][29], Y [n][20] */
+int fem_mlp_train(fem_mlp* mlp, const float* X, const float* Y, int32_t n, int32_t epochs, int32_t batch, float lr,
+                  uint64_t seed, fem_mlp_train_info* info);
+/* gradient of mean ||MLP(X) - Y||^2 w.r.t. the (BF16-rounded) weights, device grad [n_params] */
+int fem_mlp_gradient(fem_mlp* mlp, const float* X, const float* Y, int32_t n, float* grad, double* loss,
+                     void* stream);
+int fem_mlp_forward(fem_mlp* mlp, const float* X, float* O, int32_t n, void* stream);
+int fem_mlp_save(const fem_mlp* mlp, const char* path);
+int fem_mlp_load(const char* path, fem_mlp** out);
+/* use mlp on the finest level of mg (NULL: back to Chebyshev); fallback != 0
+ * re-enables Chebyshev after the first poor outer iteration */
+int fem_mg_set_learned_smoother(fem_mg* mg, fem_mlp* mlp, int32_t fallback);
 
 /* ---- batched multi-problem launch (components-batched Helmholtz etc.) ----
  * All operators must share kind, degree, precision and n_components.  One

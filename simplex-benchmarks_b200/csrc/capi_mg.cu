@@ -220,6 +220,8 @@ int fem_cg_solve(fem_cg* cg, double* x, const double* b, double rtol, int32_t ma
       info->status = si.status;
       info->initial_residual = si.r0;
       info->final_residual = si.rn;
+      info->fallback_iteration = si.fallback_iteration;
+      info->reserved = 0;
     }
     status = si.status;
   });

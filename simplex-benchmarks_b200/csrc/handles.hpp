@@ -2,6 +2,7 @@
 #pragma once
 #include <memory>
 
+#include "learned.hpp"
 #include "mesh.hpp"
 #include "mg.hpp"
 #include "operator.hpp"
@@ -17,6 +18,9 @@ struct fem_batch {
 };
 struct fem_mg {
   std::unique_ptr<sfem::Multigrid> mg;
+};
+struct fem_mlp {
+  std::unique_ptr<sfem::LearnedSmoother> s;
 };
 struct fem_cg {
   std::unique_ptr<sfem::Preconditioner> own_precond;

@@ -18,6 +18,7 @@
 #include <map>
 #include <vector>
 
+#include "learned.hpp"
 #include "mg.hpp"
 #include "ref_tables.h"
 #include "vector_kernels.cuh"
@@ -330,11 +331,15 @@ class MultigridImpl final : public Multigrid {
   std::vector<Level> levels_;
   DevBuf<double> coarse_inv_;
   int coarse_n_ = 0;
-  DevBuf<double> d_in_, d_out_, partial_, scal_;
-  cudaGraph_t graph_ = nullptr;
-  cudaGraphExec_t exec_ = nullptr;
+  DevBuf<double> d_in_, d_out_, partial_, scal_, step_;
+  DevBuf<T> cc_rhs_, cc_y_;  // coarse-correction work vectors (level below the finest)
+  cudaGraph_t graph_[2] = {nullptr, nullptr};      // [0] Chebyshev, [1] learned finest level
+  cudaGraphExec_t exec_[2] = {nullptr, nullptr};
   cudaStream_t cap_stream_ = nullptr;
   int64_t fine_m_ = 0;
+  LearnedSmoother* learned_ = nullptr;
+  bool use_learned_ = false;
+  bool fallback_enabled_ = false;
 
   MultigridImpl(const Operator& fine, const MGParams& prm) {
     params = prm;
@@ -406,6 +411,7 @@ class MultigridImpl final : public Multigrid {
     }
     partial_.alloc(kReduceBlocks);
     scal_.alloc(1);
+    step_.alloc(2);
     // smoother spectra
     for (size_t l = 1; l < levels_.size(); ++l) estimate_eigenvalues(levels_[l]);
     build_coarse();
@@ -415,10 +421,34 @@ class MultigridImpl final : public Multigrid {
   }
 
   ~MultigridImpl() override {
-    if (exec_) cudaGraphExecDestroy(exec_);
-    if (graph_) cudaGraphDestroy(graph_);
+    for (int k = 0; k < 2; ++k) {
+      if (exec_[k]) cudaGraphExecDestroy(exec_[k]);
+      if (graph_[k]) cudaGraphDestroy(graph_[k]);
+    }
     if (cap_stream_) cudaStreamDestroy(cap_stream_);
   }
+
+  void set_learned(LearnedSmoother* s, bool fallback) override {
+    if (s) {
+      const Level& top = levels_.back();
+      SFEM_REQUIRE(top.degree == 3, FEM_ERR_ARG, "learned smoother: the finest level must be P3");
+    }
+    learned_ = s;
+    use_learned_ = s != nullptr;
+    fallback_enabled_ = fallback;
+    if (exec_[1]) {
+      cudaGraphExecDestroy(exec_[1]);
+      cudaGraphDestroy(graph_[1]);
+      exec_[1] = nullptr;
+      graph_[1] = nullptr;
+    }
+  }
+  bool fallback_to_chebyshev() override {
+    if (!use_learned_ || !fallback_enabled_) return false;
+    use_learned_ = false;
+    return true;
+  }
+  bool learned_active() const override { return use_learned_; }
 
   double dot(const T* x, const T* y, int64_t n, cudaStream_t s) {
     vec_dot_partial<T><<<kReduceBlocks, kReduceThreads, 0, s>>>(n, x, y, partial_.p);
@@ -595,15 +625,77 @@ class MultigridImpl final : public Multigrid {
     }
     const int64_t m = L.op->m;
     const unsigned g = grid_for(m);
-    smooth(l, L.x.p, L.b.p, true, s);
-    L.op->vmult(L.t.p, L.x.p, s);
-    vec_residual<T><<<g, 256, 0, s>>>(m, L.b.p, L.t.p, L.r.p);
+    const bool learned = use_learned_ && l == int(levels_.size()) - 1;
+    if (learned) {
+      // pre-smoothing from zero: x = w z, z = S(b), w = (b,z)/(z,Az); r = b - w Az
+      SFEM_CUDA(cudaMemsetAsync(L.x.p, 0, sizeof(T) * m, s));
+      learned_step(L, L.b.p, s);
+      residual_ratio<T><<<g, 256, 0, s>>>(m, step_.p, L.b.p, L.t.p, L.r.p);
+    } else {
+      smooth(l, L.x.p, L.b.p, true, s);
+      L.op->vmult(L.t.p, L.x.p, s);
+      vec_residual<T><<<g, 256, 0, s>>>(m, L.b.p, L.t.p, L.r.p);
+    }
     Level& C = levels_[l - 1];
     SFEM_CUDA(cudaMemsetAsync(C.b.p, 0, sizeof(T) * C.op->m, s));
     restrict_add(l, C.b.p, L.r.p, s);
     cycle(l - 1, s);
     prolongate_add(l, L.x.p, C.x.p, s);
-    smooth(l, L.x.p, L.b.p, false, s);
+    if (learned) {
+      // post-smoothing: one energy-optimal step along S(b - A x)
+      L.op->vmult(L.t.p, L.x.p, s);
+      vec_residual<T><<<g, 256, 0, s>>>(m, L.b.p, L.t.p, L.r.p);
+      learned_step(L, L.r.p, s);
+    } else {
+      smooth(l, L.x.p, L.b.p, false, s);
+    }
+  }
+
+  // Learned smoothing step for residual r: z = S(r) (into L.d), A z (into L.t),
+  // x += w z with the energy-optimal w = (r,z)/(z,Az); step_ keeps (r,z),(z,Az)
+  // on the device so the step needs no host synchronisation (graph capturable).
+  // Any direction z with (r,z) > 0 then lowers the A-norm of the error.
+  void learned_step(Level& L, const T* r, cudaStream_t s) {
+    const int64_t m = L.op->m;
+    SFEM_CUDA(cudaMemsetAsync(L.d.p, 0, sizeof(T) * m, s));
+    learned_->apply(*L.op, r, L.d.p, s);
+    L.op->vmult(L.t.p, L.d.p, s);
+    vec_dot_partial<T><<<kReduceBlocks, kReduceThreads, 0, s>>>(m, r, L.d.p, partial_.p);
+    reduce_partials<<<1, kReduceThreads, 0, s>>>(kReduceBlocks, partial_.p, step_.p);
+    vec_dot_partial<T><<<kReduceBlocks, kReduceThreads, 0, s>>>(m, L.d.p, L.t.p, partial_.p);
+    reduce_partials<<<1, kReduceThreads, 0, s>>>(kReduceBlocks, partial_.p, step_.p + 1);
+    axpy_ratio<T><<<grid_for(m), 256, 0, s>>>(m, step_.p, L.d.p, L.x.p);
+    SFEM_CUDA(cudaGetLastError());
+  }
+
+  void on_solve_start() override { use_learned_ = learned_ != nullptr; }
+
+  void coarse_correction(const double* r, double* x, int iterations, cudaStream_t s) override {
+    const int top = int(levels_.size()) - 1;
+    SFEM_REQUIRE(top >= 1, FEM_ERR_STATE, "coarse correction needs two levels");
+    SFEM_REQUIRE(iterations >= 1, FEM_ERR_ARG, "coarse correction: iterations >= 1");
+    Level& L = levels_[top];
+    Level& C = levels_[top - 1];
+    const int64_t m = L.op->m, mc = C.op->m;
+    if (cc_rhs_.n != size_t(mc)) {
+      cc_rhs_.alloc(mc);
+      cc_y_.alloc(mc);
+    }
+    vec_convert<T, double><<<grid_for(m), 256, 0, s>>>(m, r, L.r.p);
+    SFEM_CUDA(cudaMemsetAsync(cc_rhs_.p, 0, sizeof(T) * mc, s));
+    restrict_add(top, cc_rhs_.p, L.r.p, s);
+    SFEM_CUDA(cudaMemsetAsync(cc_y_.p, 0, sizeof(T) * mc, s));
+    // y += V(R r - A_c y): V-cycle iteration on the level below
+    for (int it = 0; it < iterations; ++it) {
+      C.op->vmult(C.t.p, cc_y_.p, s);
+      vec_residual<T><<<grid_for(mc), 256, 0, s>>>(mc, cc_rhs_.p, C.t.p, C.b.p);
+      cycle(top - 1, s);
+      vec_axpby<T><<<grid_for(mc), 256, 0, s>>>(mc, T(1), C.x.p, T(1), cc_y_.p);
+    }
+    SFEM_CUDA(cudaMemsetAsync(L.x.p, 0, sizeof(T) * m, s));
+    prolongate_add(top, L.x.p, cc_y_.p, s);
+    vec_convert<double, T><<<grid_for(m), 256, 0, s>>>(m, L.x.p, x);
+    SFEM_CUDA(cudaGetLastError());
   }
 
   void run_cycle(cudaStream_t s) {
@@ -618,17 +710,18 @@ class MultigridImpl final : public Multigrid {
   void vcycle(double* dst, const double* src, cudaStream_t s) override {
     SFEM_CUDA(cudaMemcpyAsync(d_in_.p, src, sizeof(double) * fine_m_, cudaMemcpyDeviceToDevice, s));
     if (params.use_graph) {
-      if (!exec_) {
-        // one eager cycle sets up kernel attributes, then capture
+      const int mode = use_learned_ ? 1 : 0;
+      if (!exec_[mode]) {
+        // one eager cycle sets up kernel attributes and bindings, then capture
         run_cycle(s);
         SFEM_CUDA(cudaStreamSynchronize(s));
-        SFEM_CUDA(cudaStreamCreateWithFlags(&cap_stream_, cudaStreamNonBlocking));
+        if (!cap_stream_) SFEM_CUDA(cudaStreamCreateWithFlags(&cap_stream_, cudaStreamNonBlocking));
         SFEM_CUDA(cudaStreamBeginCapture(cap_stream_, cudaStreamCaptureModeThreadLocal));
         run_cycle(cap_stream_);
-        SFEM_CUDA(cudaStreamEndCapture(cap_stream_, &graph_));
-        SFEM_CUDA(cudaGraphInstantiate(&exec_, graph_, 0));
+        SFEM_CUDA(cudaStreamEndCapture(cap_stream_, &graph_[mode]));
+        SFEM_CUDA(cudaGraphInstantiate(&exec_[mode], graph_[mode], 0));
       }
-      SFEM_CUDA(cudaGraphLaunch(exec_, s));
+      SFEM_CUDA(cudaGraphLaunch(exec_[mode], s));
     } else {
       run_cycle(s);
     }
@@ -669,6 +762,7 @@ SolveInfo CGSolver::solve(double* x, const double* b, double rtol, int maxit, cu
   SolveInfo info;
   const int64_t m = A_.m;
   const unsigned g = grid_for(m);
+  if (M_) M_->on_solve_start();
   // r = b - A x
   A_.vmult(q_.p, x, s);
   vec_residual<double><<<g, 256, 0, s>>>(m, b, q_.p, r_.p);
@@ -689,6 +783,7 @@ SolveInfo CGSolver::solve(double* x, const double* b, double rtol, int maxit, cu
   precondition(z_.p, r_.p);
   SFEM_CUDA(cudaMemcpyAsync(p_.p, z_.p, sizeof(double) * m, cudaMemcpyDeviceToDevice, s));
   double rz = dot(r_.p, z_.p, s);
+  double prev_rn = info.r0;
   info.status = FEM_ERR_NOT_CONVERGED;
   for (int it = 1; it <= maxit; ++it) {
     A_.vmult(q_.p, p_.p, s);
@@ -716,6 +811,10 @@ SolveInfo CGSolver::solve(double* x, const double* b, double rtol, int maxit, cu
       info.status = FEM_OK;
       break;
     }
+    // a cycle that reduced the residual by less than 2x: fall back if the preconditioner can
+    if (M_ && !info.fallback_iteration && info.rn > 0.5 * prev_rn && M_->on_poor_reduction())
+      info.fallback_iteration = it;
+    prev_rn = info.rn;
     if (flexible_) SFEM_CUDA(cudaMemcpyAsync(zold_.p, z_.p, sizeof(double) * m, cudaMemcpyDeviceToDevice, s));
     precondition(z_.p, r_.p);
     const double rz_new = dot(r_.p, z_.p, s);

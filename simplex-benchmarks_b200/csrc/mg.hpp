@@ -44,6 +44,19 @@ class Multigrid {
   virtual void restrict_add(int l, void* dst, const void* src, cudaStream_t s) = 0;    // l -> l-1
   virtual void coarse_solve(void* dst, const void* src, cudaStream_t s) = 0;
   virtual Operator& level_operator(int l) = 0;
+  // finest-level smoothing by a learned per-cell MLP (nullptr: Chebyshev);
+  // with fallback the Chebyshev smoother returns on the first poor cycle
+  virtual void set_learned(class LearnedSmoother* s, bool fallback) = 0;
+  // switch back to Chebyshev (returns true if the learned smoother was active)
+  virtual bool fallback_to_chebyshev() = 0;
+  virtual bool learned_active() const = 0;
+  // a new outer solve starts: a learned smoother that fell back is used again
+  virtual void on_solve_start() = 0;
+  // x = P y, y ~ A_c^-1 R r by `iterations` V-cycle iterations on the level below
+  // the finest: the coarse-grid correction of the FP64 fine residual r (no
+  // finest-level smoothing); with enough iterations r - A x is A-orthogonal to
+  // the coarse space
+  virtual void coarse_correction(const double* r, double* x, int iterations, cudaStream_t s) = 0;
 };
 
 std::unique_ptr<Multigrid> make_multigrid(const Operator& fine, const MGParams& p);
@@ -52,6 +65,7 @@ struct SolveInfo {
   int iterations = 0;
   int status = 0;  // FEM_OK, FEM_ERR_NOT_CONVERGED, FEM_ERR_BREAKDOWN, FEM_ERR_NONFINITE
   double r0 = 0, rn = 0;
+  int fallback_iteration = 0;  // iteration at which a learned smoother was replaced (0: never)
 };
 
 // Preconditioner interface for the CG solver (FP64 vectors of the fine operator)
@@ -59,6 +73,10 @@ class Preconditioner {
  public:
   virtual ~Preconditioner() = default;
   virtual void apply(double* dst, const double* src, cudaStream_t s) = 0;
+  // the outer iteration reduced the residual by less than 2x: change strategy
+  // if the preconditioner has another one (returns true if it did)
+  virtual bool on_poor_reduction() { return false; }
+  virtual void on_solve_start() {}
 };
 
 class CGSolver {
@@ -80,6 +98,8 @@ class MGPreconditioner final : public Preconditioner {
  public:
   explicit MGPreconditioner(Multigrid& mg) : mg_(mg) {}
   void apply(double* dst, const double* src, cudaStream_t s) override { mg_.vcycle(dst, src, s); }
+  bool on_poor_reduction() override { return mg_.fallback_to_chebyshev(); }
+  void on_solve_start() override { mg_.on_solve_start(); }
 
  private:
   Multigrid& mg_;

@@ -58,7 +58,7 @@ __global__ void __launch_bounds__(kReduceThreads) vec_dot_partial(int64_t n, con
   if (threadIdx.x == 0) partial[blockIdx.x] = s[0];
 }
 
-__global__ void __launch_bounds__(kReduceThreads) reduce_partials(int n, const double* partial, double* out) {
+static __global__ void __launch_bounds__(kReduceThreads) reduce_partials(int n, const double* partial, double* out) {
   __shared__ double s[kReduceThreads];
   double acc = 0.0;
   for (int i = threadIdx.x; i < n; i += blockDim.x) acc += partial[i];
@@ -119,12 +119,31 @@ __global__ void dense_matvec(int n, const double* __restrict__ A, const T* __res
 }
 
 // PCG update: x += alpha p, r -= alpha q
-__global__ void cg_update_xr(int64_t n, double alpha, const double* __restrict__ p, const double* __restrict__ q,
+static __global__ void cg_update_xr(int64_t n, double alpha, const double* __restrict__ p, const double* __restrict__ q,
                              double* __restrict__ x, double* __restrict__ r) {
   for (int64_t i = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; i < n; i += int64_t(gridDim.x) * blockDim.x) {
     x[i] += alpha * p[i];
     r[i] -= alpha * q[i];
   }
+}
+
+// x += (sc[0]/sc[1]) z  (step 0 unless sc[1] > 0); the ratio stays on the device
+template <typename T>
+__global__ void axpy_ratio(int64_t n, const double* __restrict__ sc, const T* __restrict__ z, T* __restrict__ x) {
+  const double den = sc[1];
+  const T w = den > 0.0 ? T(sc[0] / den) : T(0);
+  for (int64_t i = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; i < n; i += int64_t(gridDim.x) * blockDim.x)
+    x[i] += w * z[i];
+}
+
+// r = b - (sc[0]/sc[1]) q
+template <typename T>
+__global__ void residual_ratio(int64_t n, const double* __restrict__ sc, const T* __restrict__ b,
+                               const T* __restrict__ q, T* __restrict__ r) {
+  const double den = sc[1];
+  const T w = den > 0.0 ? T(sc[0] / den) : T(0);
+  for (int64_t i = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; i < n; i += int64_t(gridDim.x) * blockDim.x)
+    r[i] = b[i] - w * q[i];
 }
 
 inline unsigned grid_for(int64_t n, int bs = 256, unsigned cap = 148 * 16) {

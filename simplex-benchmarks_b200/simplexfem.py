@@ -53,7 +53,19 @@ class MGParams(C.Structure):
 
 class SolveInfo(C.Structure):
     _fields_ = [("iterations", C.c_int32), ("status", C.c_int32), ("initial_residual", C.c_double),
-                ("final_residual", C.c_double)]
+                ("final_residual", C.c_double), ("fallback_iteration", C.c_int32), ("reserved", C.c_int32)]
+
+
+class MLPTrainParams(C.Structure):
+    _fields_ = [("n_sizes", C.c_int32), ("sizes", C.c_int32 * 4), ("rhs_per_size", C.c_int32),
+                ("iterates", C.c_int32), ("samples", C.c_int32), ("epochs", C.c_int32), ("batch", C.c_int32),
+                ("lr", C.c_float), ("jitter", C.c_double), ("seed", C.c_uint64), ("noise_fraction", C.c_double),
+                ("coarse_iterations", C.c_int32), ("reserved", C.c_int32)]
+
+
+class MLPTrainInfo(C.Structure):
+    _fields_ = [("samples", C.c_int32), ("reserved", C.c_int32), ("loss_first", C.c_double),
+                ("loss_last", C.c_double), ("seconds", C.c_double)]
 
 
 FEM_RHS_PLANE_WAVES, FEM_RHS_SINE_PRODUCTS = 0, 1
@@ -109,6 +121,21 @@ _PROTOS = [
     ("fem_cg_destroy", C.c_int, [C.c_void_p]),
     ("fem_cg_solve", C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_double, C.c_int32,
                                C.POINTER(SolveInfo), C.c_void_p]),
+    ("fem_mlp_create", C.c_int, [C.c_uint64, C.POINTER(C.c_void_p)]),
+    ("fem_mlp_destroy", C.c_int, [C.c_void_p]),
+    ("fem_mlp_n_params", C.c_int, [C.POINTER(C.c_int32)]),
+    ("fem_mlp_get_weights", C.c_int, [C.c_void_p, C.c_void_p]),
+    ("fem_mlp_set_weights", C.c_int, [C.c_void_p, C.c_void_p]),
+    ("fem_mlp_train_params_default", C.c_int, [C.POINTER(MLPTrainParams)]),
+    ("fem_mlp_generate_and_train", C.c_int, [C.c_void_p, C.POINTER(MLPTrainParams), C.POINTER(MLPTrainInfo)]),
+    ("fem_mlp_train", C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_int32, C.c_int32, C.c_int32, C.c_float,
+                                C.c_uint64, C.POINTER(MLPTrainInfo)]),
+    ("fem_mlp_gradient", C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_int32, C.c_void_p,
+                                   C.POINTER(C.c_double), C.c_void_p]),
+    ("fem_mlp_forward", C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_int32, C.c_void_p]),
+    ("fem_mlp_save", C.c_int, [C.c_void_p, C.c_char_p]),
+    ("fem_mlp_load", C.c_int, [C.c_char_p, C.POINTER(C.c_void_p)]),
+    ("fem_mg_set_learned_smoother", C.c_int, [C.c_void_p, C.c_void_p, C.c_int32]),
     ("fem_batch_create", C.c_int, [C.c_void_p, C.c_int32, C.POINTER(C.c_void_p)]),
     ("fem_batch_destroy", C.c_int, [C.c_void_p]),
     ("fem_batch_vmult", C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]),
@@ -397,6 +424,12 @@ class Multigrid:
     def coarse_solve(self, dst, src, stream=None):
         check(lib().fem_mg_coarse_solve(self.handle, _ptr(dst), _ptr(src), _stream_ptr(stream)))
 
+    def set_learned_smoother(self, mlp, fallback=True):
+        """Finest-level smoothing by a trained MLP (None: back to Chebyshev)."""
+        self.mlp = mlp
+        check(lib().fem_mg_set_learned_smoother(self.handle, mlp.handle if mlp is not None else None,
+                                                int(bool(fallback))))
+
     def __del__(self):
         if getattr(self, "handle", None) and _lib is not None:
             _lib.fem_mg_destroy(self.handle)
@@ -427,9 +460,84 @@ class SolverCG:
                 raise_on_failure and rc != FEM_OK):
             check(rc)
         return {"iterations": info.iterations, "status": info.status, "r0": info.initial_residual,
-                "rn": info.final_residual}
+                "rn": info.final_residual, "fallback_iteration": info.fallback_iteration}
 
     def __del__(self):
         if getattr(self, "handle", None) and _lib is not None:
             _lib.fem_cg_destroy(self.handle)
+            self.handle = None
+
+
+def mlp_n_params():
+    n = C.c_int32()
+    check(lib().fem_mlp_n_params(C.byref(n)))
+    return n.value
+
+
+class MLP:
+    """Learned finest-level smoother (fem_mlp): 29 -> 64 -> 64 -> 20, GELU, BF16 weights."""
+
+    def __init__(self, seed=0, handle=None):
+        if handle is None:
+            handle = C.c_void_p()
+            check(lib().fem_mlp_create(seed, C.byref(handle)))
+        self.handle = handle
+
+    @classmethod
+    def load(cls, path):
+        h = C.c_void_p()
+        check(lib().fem_mlp_load(str(path).encode(), C.byref(h)))
+        return cls(handle=h)
+
+    def save(self, path):
+        check(lib().fem_mlp_save(self.handle, str(path).encode()))
+
+    def weights(self):
+        w = np.empty(mlp_n_params(), np.float32)
+        check(lib().fem_mlp_get_weights(self.handle, w.ctypes.data))
+        return w
+
+    def set_weights(self, w):
+        w = np.ascontiguousarray(w, np.float32)
+        assert w.size == mlp_n_params()
+        check(lib().fem_mlp_set_weights(self.handle, w.ctypes.data))
+
+    def generate_and_train(self, **kw):
+        p = MLPTrainParams()
+        check(lib().fem_mlp_train_params_default(C.byref(p)))
+        for k, v in kw.items():
+            if k == "sizes":
+                p.n_sizes = len(v)
+                for i, s in enumerate(v):
+                    p.sizes[i] = s
+            else:
+                setattr(p, k, v)
+        info = MLPTrainInfo()
+        check(lib().fem_mlp_generate_and_train(self.handle, C.byref(p), C.byref(info)))
+        return {"samples": info.samples, "loss_first": info.loss_first, "loss_last": info.loss_last,
+                "seconds": info.seconds}
+
+    def train(self, X, Y, epochs=10, batch=256, lr=1e-3, seed=0):
+        info = MLPTrainInfo()
+        check(lib().fem_mlp_train(self.handle, _ptr(X), _ptr(Y), X.shape[0], epochs, batch, lr, seed,
+                                  C.byref(info)))
+        return {"loss_first": info.loss_first, "loss_last": info.loss_last}
+
+    def gradient(self, X, Y, stream=None):
+        import torch
+        g = torch.zeros(mlp_n_params(), dtype=torch.float32, device="cuda")
+        loss = C.c_double()
+        check(lib().fem_mlp_gradient(self.handle, _ptr(X), _ptr(Y), X.shape[0], _ptr(g), C.byref(loss),
+                                     _stream_ptr(stream)))
+        return g, loss.value
+
+    def forward(self, X, stream=None):
+        import torch
+        O = torch.zeros((X.shape[0], 20), dtype=torch.float32, device="cuda")
+        check(lib().fem_mlp_forward(self.handle, _ptr(X), _ptr(O), X.shape[0], _stream_ptr(stream)))
+        return O
+
+    def __del__(self):
+        if getattr(self, "handle", None) and _lib is not None:
+            _lib.fem_mlp_destroy(self.handle)
             self.handle = None

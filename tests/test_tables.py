@@ -62,3 +62,24 @@ def test_face_node_lists_lie_on_faces(tables, p):
         for n in tables[p]["FN"][f]:
             assert lat[n][f] == 0
         assert len(tables[p]["FN"][f]) == (p + 1) * (p + 2) // 2
+
+
+def test_mlp_oracle_gradient_is_the_derivative():
+    """Pin of the MLP oracle: its gradient matches central finite differences."""
+    import mlp_oracle
+    rng = np.random.default_rng(0)
+    w = (rng.standard_normal(mlp_oracle.NPARAM) * 0.2).astype(np.float32)
+    w = mlp_oracle.bf16_round(w)  # exactly representable, so rounding is the identity
+    X = rng.standard_normal((8, 29))
+    Y = rng.standard_normal((8, 20))
+    _, g = mlp_oracle.loss_and_grad(w, X, Y)
+    for i in rng.choice(mlp_oracle.NPARAM, 12, replace=False):
+        # step of one bf16 ulp pair around w[i] keeps the rounded weights exact
+        wp, wm = w.copy(), w.copy()
+        h = max(abs(float(w[i])), 1e-3) * 2 ** -7
+        wp[i] = mlp_oracle.bf16_round(np.array([w[i] + h], np.float32))[0]
+        wm[i] = mlp_oracle.bf16_round(np.array([w[i] - h], np.float32))[0]
+        lp, _ = mlp_oracle.loss_and_grad(wp, X, Y)
+        lm, _ = mlp_oracle.loss_and_grad(wm, X, Y)
+        fd = (lp - lm) / (float(wp[i]) - float(wm[i]))
+        assert abs(fd - g[i]) <= 2e-2 * max(1e-3, abs(g[i])) + 1e-6, (i, fd, g[i])
