@@ -284,6 +284,15 @@ int fem_mlp_train(fem_mlp* mlp, const float* X, const float* Y, int32_t n, int32
 int fem_mlp_gradient(fem_mlp* mlp, const float* X, const float* Y, int32_t n, float* grad, double* loss,
                      void* stream);
 int fem_mlp_forward(fem_mlp* mlp, const float* X, float* O, int32_t n, void* stream);
+/* The same forward on the tensor cores (tcgen05 MMAs, BF16 operands, FP32
+ * accumulators, BF16 activations between the layers): the kernel the
+ * smoother uses when tensor cores are on.  No counterpart in the reference. */
+int fem_mlp_forward_tc(fem_mlp* mlp, const float* X, float* O, int32_t n, void* stream);
+/* smoothing on the tensor cores (on != 0, default) or on the CUDA cores */
+int fem_mlp_set_tensor_cores(fem_mlp* mlp, int32_t on);
+/* *timed_out = 1 if a tensor-core launch gave up on a bounded wait since the
+ * last call (the results of that launch are then invalid); synchronises */
+int fem_mlp_status(fem_mlp* mlp, int32_t* timed_out);
 int fem_mlp_save(const fem_mlp* mlp, const char* path);
 int fem_mlp_load(const char* path, fem_mlp** out);
 /* use mlp on the finest level of mg (NULL: back to Chebyshev); fallback != 0

@@ -1,13 +1,12 @@
 """FP64 numpy restatement of the learned smoother's MLP (test infrastructure).
 
-Forward and backward of 29 -> 64 -> 64 -> 20 with exact GELU, on the BF16
+Forward and backward of 29 -> 64 -> 64 -> 20 with the tanh-form GELU, on the BF16
 rounding of the weights (the product computes with BF16 weights and FP32
 accumulation), and the loss mean_b ||o_b - y_b||^2.  Used as the oracle of
 the GPU gradient kernels.  Parameter layout:
 W1 [64][29], b1 [64], W2 [64][64], b2 [64], W3 [20][64], b3 [20].
 """
 import numpy as np
-from scipy.special import erf
 
 NIN, NH, NOUT = 29, 64, 20
 SHAPES = [("W1", (NH, NIN)), ("b1", (NH,)), ("W2", (NH, NH)), ("b2", (NH,)), ("W3", (NOUT, NH)), ("b3", (NOUT,))]
@@ -31,20 +30,28 @@ def unpack(w):
     return out
 
 
+C_GELU = np.sqrt(2 / np.pi)
+
+
 def gelu(x):
-    return 0.5 * x * (1 + erf(x / np.sqrt(2)))
+    """GELU, tanh form: 0.5 x (1 + tanh(sqrt(2/pi) (x + 0.044715 x^3)))."""
+    return 0.5 * x * (1 + np.tanh(C_GELU * (x + 0.044715 * x ** 3)))
 
 
 def gelu_grad(x):
-    return 0.5 * (1 + erf(x / np.sqrt(2))) + x * np.exp(-0.5 * x * x) / np.sqrt(2 * np.pi)
+    t = np.tanh(C_GELU * (x + 0.044715 * x ** 3))
+    return 0.5 * (1 + t) + 0.5 * x * (1 - t * t) * C_GELU * (1 + 3 * 0.044715 * x * x)
 
 
-def forward(w, X):
+def forward(w, X, bf16_activations=False):
+    """bf16_activations: round the inputs and both hidden activations to BF16,
+    as the tensor-core path does (its MMA operands are BF16)."""
     p = unpack(bf16_round(w))
-    a1 = X @ p["W1"].T + p["b1"]
-    h1 = gelu(a1)
+    r = (lambda a: bf16_round(np.asarray(a, np.float32)).astype(np.float64)) if bf16_activations else (lambda a: a)
+    a1 = r(X) @ p["W1"].T + p["b1"]
+    h1 = r(gelu(a1))
     a2 = h1 @ p["W2"].T + p["b2"]
-    h2 = gelu(a2)
+    h2 = r(gelu(a2))
     return h2 @ p["W3"].T + p["b3"], (a1, h1, a2, h2, p)
 
 

@@ -136,6 +136,30 @@ int fem_mlp_forward(fem_mlp* mlp, const float* X, float* O, int32_t n, void* str
   });
 }
 
+int fem_mlp_forward_tc(fem_mlp* mlp, const float* X, float* O, int32_t n, void* stream) {
+  return guarded([&] {
+    SFEM_REQUIRE_PTR(mlp);
+    SFEM_REQUIRE_PTR(X);
+    SFEM_REQUIRE_PTR(O);
+    mlp->s->forward_tc(X, O, n, static_cast<cudaStream_t>(stream));
+  });
+}
+
+int fem_mlp_set_tensor_cores(fem_mlp* mlp, int32_t on) {
+  return guarded([&] {
+    SFEM_REQUIRE_PTR(mlp);
+    mlp->s->set_tensor_cores(on != 0);
+  });
+}
+
+int fem_mlp_status(fem_mlp* mlp, int32_t* timed_out) {
+  return guarded([&] {
+    SFEM_REQUIRE_PTR(mlp);
+    SFEM_REQUIRE_PTR(timed_out);
+    *timed_out = mlp->s->status(true);
+  });
+}
+
 int fem_mlp_save(const fem_mlp* mlp, const char* path) {
   return guarded([&] {
     SFEM_REQUIRE_PTR(mlp);

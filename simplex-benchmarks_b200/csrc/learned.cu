@@ -12,6 +12,7 @@
 #include "learned.hpp"
 #include "mg.hpp"
 #include "mlp.cuh"
+#include "mlp_tc.cuh"
 #include "vector_kernels.cuh"
 
 namespace sfem {
@@ -24,6 +25,26 @@ __global__ void gather_rows(int n, int width, const int32_t* __restrict__ perm, 
   if (t >= int64_t(n) * width) return;
   const int64_t r = t / width, c = t % width;
   out[t] = in[int64_t(perm[r]) * width + c];
+}
+
+// persistent tensor-core launch: at most 4 CTAs per SM (each holds 64
+// tensor-memory columns and 41 KB of shared memory)
+template <int MODE, typename T>
+void launch_tc(int64_t n, const int32_t* dofs, const float* feat, const float* winv, const __nv_bfloat16* wb,
+               const T* r, T* z, float* zout, int* status, cudaStream_t s) {
+  static bool configured = false;
+  auto kern = mlp_tc_kernel<MODE, T>;
+  if (!configured) {
+    SFEM_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, tc::SMEM_BYTES));
+    configured = true;
+  }
+  int dev = 0, sms = 0;
+  SFEM_CUDA(cudaGetDevice(&dev));
+  SFEM_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+  const int64_t tiles = (n + tc::TILE - 1) / tc::TILE;
+  const unsigned grid = unsigned(std::max<int64_t>(1, std::min<int64_t>(tiles, int64_t(sms) * 4)));
+  kern<<<grid, 128, tc::SMEM_BYTES, s>>>(n, dofs, feat, winv, wb, r, z, zout, status);
+  SFEM_CUDA(cudaGetLastError());
 }
 
 uint64_t fnv1a(const void* data, size_t n) {
@@ -58,6 +79,8 @@ LearnedSmoother::LearnedSmoother(uint64_t seed) {
   g_.alloc(NP);
   loss_.alloc(1);
   wb_.alloc(NP);
+  status_.alloc(1);
+  SFEM_CUDA(cudaMemset(status_.p, 0, sizeof(int)));
   set_weights(w);
 }
 
@@ -110,6 +133,15 @@ LearnedSmoother::Bound& LearnedSmoother::bind(const Operator& op) {
 
 void LearnedSmoother::apply(const Operator& op, const void* r, void* z, cudaStream_t s) {
   Bound& b = bind(op);
+  if (tensor_cores_) {
+    if (op.cfg.precision == FEM_FP64)
+      launch_tc<0, double>(op.n_cells, op.device_dof_table(), b.feat.p, b.winv.p, wb_.p,
+                           static_cast<const double*>(r), static_cast<double*>(z), nullptr, status_.p, s);
+    else
+      launch_tc<0, float>(op.n_cells, op.device_dof_table(), b.feat.p, b.winv.p, wb_.p,
+                          static_cast<const float*>(r), static_cast<float*>(z), nullptr, status_.p, s);
+    return;
+  }
   const unsigned grid = unsigned(std::min<int64_t>((op.n_cells + 127) / 128, 148 * 8));
   if (op.cfg.precision == FEM_FP64)
     mlp_smooth_kernel<double><<<grid, 128, 0, s>>>(op.n_cells, op.device_dof_table(), b.feat.p, b.winv.p, wb_.p,
@@ -142,6 +174,18 @@ void LearnedSmoother::forward(const float* X, float* O, int n, cudaStream_t s) {
   const int grid = std::max(1, std::min((n + 127) / 128, 148 * 8));
   mlp_forward_kernel<<<grid, 128, 0, s>>>(n, X, wb_.p, O);
   SFEM_CUDA(cudaGetLastError());
+}
+
+void LearnedSmoother::forward_tc(const float* X, float* O, int n, cudaStream_t s) {
+  SFEM_REQUIRE(n >= 0, FEM_ERR_ARG, "mlp: negative sample count");
+  launch_tc<1, float>(n, nullptr, X, nullptr, wb_.p, nullptr, nullptr, O, status_.p, s);
+}
+
+int LearnedSmoother::status(bool clear) {
+  int v = 0;
+  SFEM_CUDA(cudaMemcpy(&v, status_.p, sizeof(int), cudaMemcpyDeviceToHost));
+  if (clear && v) SFEM_CUDA(cudaMemset(status_.p, 0, sizeof(int)));
+  return v;
 }
 
 TrainStats LearnedSmoother::train(const float* X, const float* Y, int n, int epochs, int batch, float lr,

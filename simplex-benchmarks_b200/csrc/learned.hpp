@@ -54,6 +54,13 @@ class LearnedSmoother {
   // gradient of mean ||o - y||^2 over n samples (device arrays); grad on device [NP]
   double gradient(const float* X, const float* Y, int n, float* grad, cudaStream_t s);
   void forward(const float* X, float* O, int n, cudaStream_t s);
+  // the same forward on the tensor cores (tcgen05, BF16 activations)
+  void forward_tc(const float* X, float* O, int n, cudaStream_t s);
+  // smoothing on the tensor cores (default) or on the CUDA cores
+  void set_tensor_cores(bool on) { tensor_cores_ = on; }
+  bool tensor_cores() const { return tensor_cores_; }
+  // 1 if a tensor-core launch gave up on a bounded wait since the last call
+  int status(bool clear);
   void save(const std::string& path) const;
   static std::unique_ptr<LearnedSmoother> load(const std::string& path);
   const __nv_bfloat16* bf16() const { return wb_.p; }
@@ -67,6 +74,8 @@ class LearnedSmoother {
   void round_weights(cudaStream_t s);
   DevBuf<float> w_, m_, v_, g_, loss_;
   DevBuf<__nv_bfloat16> wb_;
+  DevBuf<int> status_;
+  bool tensor_cores_ = true;
   int adam_t_ = 0;
   std::map<const Operator*, std::unique_ptr<Bound>> bound_;
 };

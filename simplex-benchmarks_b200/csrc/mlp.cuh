@@ -1,4 +1,4 @@
-// Per-cell MLP of the learned smoother: 29 -> 64 -> 64 -> 20, GELU, BF16
+// Per-cell MLP of the learned smoother: 29 -> 64 -> 64 -> 20, GELU (tanh form), BF16
 // weights, FP32 accumulation.  No counterpart in the reference (its finest
 // level is always smoothed by PreconditionChebyshev).
 //
@@ -21,9 +21,22 @@
 
 namespace sfem {
 
-__device__ __forceinline__ float gelu(float x) { return 0.5f * x * (1.0f + erff(x * 0.70710678118654752f)); }
+// GELU in its tanh form, 0.5 x (1 + tanh(sqrt(2/pi) (x + 0.044715 x^3)))
+// (Hendrycks & Gimpel), and its derivative.
+__device__ __forceinline__ float gelu(float x) {
+  const float u = 0.7978845608028654f * (x + 0.044715f * x * x * x);
+  return 0.5f * x * (1.0f + tanhf(u));
+}
 __device__ __forceinline__ float gelu_grad(float x) {
-  return 0.5f * (1.0f + erff(x * 0.70710678118654752f)) + x * 0.39894228040143268f * expf(-0.5f * x * x);
+  const float t = tanhf(0.7978845608028654f * (x + 0.044715f * x * x * x));
+  return 0.5f * (1.0f + t) + 0.5f * x * (1.0f - t * t) * 0.7978845608028654f * (1.0f + 0.134145f * x * x);
+}
+// the same GELU with the hardware tanh approximation (tensor-core epilogues)
+__device__ __forceinline__ float gelu_fast(float x) {
+  const float u = 0.7978845608028654f * (x + 0.044715f * x * x * x);
+  float t;
+  asm("tanh.approx.f32 %0, %1;" : "=f"(t) : "f"(u));
+  return 0.5f * x * (1.0f + t);
 }
 
 // FP32 master -> BF16 image

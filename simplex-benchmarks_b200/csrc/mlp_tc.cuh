@@ -1,0 +1,299 @@
+// Tensor-core (tcgen05) inference of the learned smoother's MLP, sm_100a.
+//
+// A CTA of 128 threads owns a tile of 128 cells: the MMA's M dimension.
+// Thread t builds row t of the BF16 input tile in shared memory (the
+// normalised residual of cell t plus J/h, padded 29 -> 32).  Thread 0 issues
+// the tcgen05.mma instructions of each layer (BF16 operands from shared
+// memory, FP32 accumulators in tensor memory) and commits them to an
+// mbarrier.  Every thread then reads its own accumulator row back with
+// tcgen05.ld, adds the bias, applies GELU (tanh form, hardware tanh) and
+// writes the BF16 activation row that feeds the next layer:
+//
+//   layer 1: [128 x 32] x W1^T [32 x 64]   (2 MMAs of K = 16)
+//   layer 2: [128 x 64] x W2^T [64 x 64]   (4 MMAs)
+//   layer 3: [128 x 64] x W3^T [64 x 32]   (4 MMAs; outputs 20..31 are padding)
+//
+// The weights stay in shared memory for the CTA's lifetime (persistent grid).
+// Operand layout: K-major, no swizzle.  A core matrix is 8 rows x 16 bytes;
+// for an R-row operand, element (row, k) lives at byte
+//   (k / 8) * (R * 16) + row * 16 + (k % 8) * 2,
+// so adjacent core matrices along K are R * 16 bytes apart (leading byte
+// offset) and adjacent 8-row groups 128 bytes apart (stride byte offset).
+//
+// MODE 0: fused smoother, z += (s_K / h_K) * winv * MLP(r_K / s_K, J_K / h_K)
+//         (the same map as mlp_smooth_kernel, computed with BF16 activations).
+// MODE 1: dense forward O [n][20] = MLP(X [n][29]), used to test the kernel.
+//
+// Every mbarrier wait is bounded; on a timeout the CTA sets *status, waits
+// (bounded) for its MMAs in flight, frees its tensor memory and returns.
+#pragma once
+#include <cuda_bf16.h>
+
+#include <cstdint>
+
+#include "mlp.cuh"
+#include "mlp_dims.hpp"
+
+namespace sfem {
+namespace tc {
+
+constexpr int TILE = 128;       // cells per tile (MMA M)
+constexpr int K1 = 32;          // 29 inputs padded to a multiple of 16
+constexpr int N3 = 32;          // 20 outputs padded to a multiple of 16
+constexpr int TMEM_COLS = 64;   // one FP32 accumulator of up to 64 columns, reused by the layers
+constexpr int OFF_X = 0;                          // input tile  [128 x 32] bf16
+constexpr int OFF_H = OFF_X + TILE * K1 * 2;      // activations [128 x 64] bf16
+constexpr int OFF_W1 = OFF_H + TILE * 64 * 2;     // W1 [64 x 32]
+constexpr int OFF_W2 = OFF_W1 + 64 * K1 * 2;      // W2 [64 x 64]
+constexpr int OFF_W3 = OFF_W2 + 64 * 64 * 2;      // W3 [32 x 64]
+constexpr int OFF_B = OFF_W3 + N3 * 64 * 2;       // b1[64], b2[64], b3[32] as float
+constexpr int OFF_BAR = OFF_B + 160 * 4;          // mbarrier (8 B) + tensor-memory address (4 B)
+constexpr int SMEM_BYTES = OFF_BAR + 16;
+constexpr uint32_t kWaitLimit = 1u << 24;         // polls before a wait reports a timeout
+
+__device__ __forceinline__ uint32_t smem_u32(const void* p) {
+  return static_cast<uint32_t>(__cvta_generic_to_shared(p));
+}
+
+__device__ __forceinline__ int kmajor_off(int row, int k, int R) { return (k >> 3) * (R * 16) + row * 16 + (k & 7) * 2; }
+
+// shared-memory matrix descriptor: start, leading / stride byte offsets,
+// fixed version field 0b001 at bit 46, no swizzle
+__device__ __forceinline__ uint64_t smem_desc(uint32_t addr, uint32_t lbo, uint32_t sbo) {
+  return uint64_t((addr >> 4) & 0x3FFFu) | (uint64_t((lbo >> 4) & 0x3FFFu) << 16) |
+         (uint64_t((sbo >> 4) & 0x3FFFu) << 32) | (uint64_t(1) << 46);
+}
+
+// instruction descriptor of kind::f16: FP32 accumulator, BF16 A and B, both K-major
+__host__ __device__ constexpr uint32_t idesc_bf16(int M, int N) {
+  return (1u << 4) | (1u << 7) | (1u << 10) | (uint32_t(N >> 3) << 17) | (uint32_t(M >> 4) << 24);
+}
+
+__device__ __forceinline__ void mma_bf16(uint32_t d_tmem, uint64_t da, uint64_t db, uint32_t idesc, uint32_t acc) {
+  asm volatile(
+      "{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\t"
+      "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t}\n" ::"r"(d_tmem),
+      "l"(da), "l"(db), "r"(idesc), "r"(acc)
+      : "memory");
+}
+
+__device__ __forceinline__ void mma_commit(uint32_t bar) {
+  asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(bar)
+               : "memory");
+}
+
+__device__ __forceinline__ bool bar_wait(uint32_t bar, uint32_t phase) {
+  for (uint32_t it = 0; it < kWaitLimit; ++it) {
+    uint32_t done;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+        "selp.u32 %0, 1, 0, p;\n\t}\n"
+        : "=r"(done)
+        : "r"(bar), "r"(phase)
+        : "memory");
+    if (done) return true;
+  }
+  return false;
+}
+
+// 32 consecutive FP32 accumulator columns of this thread's row
+__device__ __forceinline__ void tmem_ld32(uint32_t taddr, float (&v)[32]) {
+  uint32_t r[32];
+  asm volatile(
+      "tcgen05.ld.sync.aligned.32x32b.x32.b32 "
+      "{%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, %15, "
+      "%16, %17, %18, %19, %20, %21, %22, %23, %24, %25, %26, %27, %28, %29, %30, %31}, [%32];"
+      : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
+        "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15]),
+        "=r"(r[16]), "=r"(r[17]), "=r"(r[18]), "=r"(r[19]), "=r"(r[20]), "=r"(r[21]), "=r"(r[22]), "=r"(r[23]),
+        "=r"(r[24]), "=r"(r[25]), "=r"(r[26]), "=r"(r[27]), "=r"(r[28]), "=r"(r[29]), "=r"(r[30]), "=r"(r[31])
+      : "r"(taddr));
+  asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+#pragma unroll
+  for (int i = 0; i < 32; ++i) v[i] = __uint_as_float(r[i]);
+}
+
+__device__ __forceinline__ void fence_async_smem() { asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); }
+__device__ __forceinline__ void tc_before_sync() { asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory"); }
+__device__ __forceinline__ void tc_after_sync() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }
+
+// 8 values of one row as one 16-byte K chunk (bf16) of an R-row operand
+__device__ __forceinline__ void store_chunk(unsigned char* base, int row, int c, int R, const float* v) {
+  __align__(16) __nv_bfloat162 p[4];
+#pragma unroll
+  for (int i = 0; i < 4; ++i) p[i] = __floats2bfloat162_rn(v[2 * i], v[2 * i + 1]);
+  *reinterpret_cast<uint4*>(base + c * (R * 16) + row * 16) = *reinterpret_cast<const uint4*>(p);
+}
+
+// issue the K / 16 MMAs of one layer: A [128 x K] at a_off, B [N x K] at b_off
+__device__ __forceinline__ void issue_layer(const unsigned char* smem, uint32_t tmem, int a_off, int b_off, int K,
+                                            int N, uint32_t bar) {
+  const uint32_t base = smem_u32(smem);
+  const uint32_t idesc = idesc_bf16(TILE, N);
+  for (int kk = 0; kk < K / 16; ++kk) {
+    const uint64_t da = smem_desc(base + a_off + kk * 2 * (TILE * 16), TILE * 16, 128);
+    const uint64_t db = smem_desc(base + b_off + kk * 2 * (N * 16), N * 16, 128);
+    mma_bf16(tmem, da, db, idesc, kk > 0 ? 1u : 0u);
+  }
+  mma_commit(bar);
+}
+
+}  // namespace tc
+
+// MODE 0 (smoother): dofs [20][n] (-1 at constrained DoFs), feat [n][10]
+// (J/h and 1/h), winv [m], r in, z += correction.  MODE 1: X [n][29] in
+// (passed as feat), O [n][20] out (passed as zout); dofs/winv/r unused.
+template <int MODE, typename T>
+__global__ void __launch_bounds__(128, 1) mlp_tc_kernel(int64_t n, const int32_t* __restrict__ dofs,
+                                                        const float* __restrict__ feat,
+                                                        const float* __restrict__ winv,
+                                                        const __nv_bfloat16* __restrict__ wb,
+                                                        const T* __restrict__ r, T* __restrict__ z,
+                                                        float* __restrict__ zout, int* __restrict__ status) {
+  using D = MLPDims;
+  using namespace tc;
+  extern __shared__ __align__(1024) unsigned char smem[];
+  float* sb = reinterpret_cast<float*>(smem + OFF_B);
+  uint64_t* bar_p = reinterpret_cast<uint64_t*>(smem + OFF_BAR);
+  uint32_t* tslot = reinterpret_cast<uint32_t*>(smem + OFF_BAR + 8);
+  const int t = threadIdx.x, warp = t >> 5;
+  const uint32_t bar = smem_u32(bar_p);
+
+  // weights -> shared memory (K-major, zero padding), biases as float
+  for (int i = t; i < 64 * K1; i += 128) {
+    const int nn = i / K1, k = i % K1;
+    const __nv_bfloat16 v = k < D::NIN ? wb[D::OFF_W1 + nn * D::NIN + k] : __float2bfloat16(0.0f);
+    *reinterpret_cast<__nv_bfloat16*>(smem + OFF_W1 + kmajor_off(nn, k, 64)) = v;
+  }
+  for (int i = t; i < 64 * 64; i += 128) {
+    const int nn = i / 64, k = i % 64;
+    *reinterpret_cast<__nv_bfloat16*>(smem + OFF_W2 + kmajor_off(nn, k, 64)) = wb[D::OFF_W2 + nn * 64 + k];
+  }
+  for (int i = t; i < N3 * 64; i += 128) {
+    const int nn = i / 64, k = i % 64;
+    const __nv_bfloat16 v = nn < D::NOUT ? wb[D::OFF_W3 + nn * 64 + k] : __float2bfloat16(0.0f);
+    *reinterpret_cast<__nv_bfloat16*>(smem + OFF_W3 + kmajor_off(nn, k, N3)) = v;
+  }
+  for (int i = t; i < 160; i += 128)
+    sb[i] = i < 64 ? __bfloat162float(wb[D::OFF_B1 + i])
+            : i < 128 ? __bfloat162float(wb[D::OFF_B2 + i - 64])
+            : i < 128 + D::NOUT ? __bfloat162float(wb[D::OFF_B3 + i - 128]) : 0.0f;
+  if (t == 0) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(bar) : "memory");
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  if (warp == 0) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(tslot)),
+                 "r"(uint32_t(TMEM_COLS))
+                 : "memory");
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+  }
+  fence_async_smem();
+  tc_before_sync();
+  __syncthreads();
+  tc_after_sync();
+  const uint32_t tmem = *tslot;
+  const uint32_t trow = tmem + (uint32_t(warp * 32) << 16);  // this warp's 32 accumulator lanes
+
+  uint32_t phase = 0;
+  bool failed = false;
+  const int64_t n_tiles = (n + TILE - 1) / TILE;
+  for (int64_t tile = blockIdx.x; tile < n_tiles; tile += gridDim.x) {
+    const int64_t c = tile * TILE + t;
+    const bool live = c < n;
+    // ---- input row
+    float x[K1];
+    int32_t g[D::NR];
+    float scale = 0.0f;
+#pragma unroll
+    for (int i = 0; i < K1; ++i) x[i] = 0.0f;
+    if (MODE == 0) {
+      float s2 = 0.0f;
+#pragma unroll
+      for (int i = 0; i < D::NR; ++i) {
+        g[i] = live ? __ldg(dofs + i * n + c) : -1;
+        x[i] = g[i] >= 0 ? float(r[g[i]]) : 0.0f;
+        s2 += x[i] * x[i];
+      }
+      if (s2 > 0.0f) {
+        const float s = sqrtf(s2), is = 1.0f / s;
+#pragma unroll
+        for (int i = 0; i < D::NR; ++i) x[i] *= is;
+#pragma unroll
+        for (int k = 0; k < D::NJ; ++k) x[D::NR + k] = __ldg(feat + c * 10 + k);
+        scale = s * __ldg(feat + c * 10 + 9);
+      } else {
+#pragma unroll
+        for (int i = 0; i < D::NR; ++i) x[i] = 0.0f;
+      }
+    } else if (live) {
+#pragma unroll
+      for (int i = 0; i < D::NIN; ++i) x[i] = __ldg(feat + c * D::NIN + i);
+    }
+#pragma unroll
+    for (int ch = 0; ch < K1 / 8; ++ch) store_chunk(smem + OFF_X, t, ch, TILE, x + 8 * ch);
+
+    // ---- three layers
+    float v[64];
+#pragma unroll 1
+    for (int layer = 0; layer < 3; ++layer) {
+      fence_async_smem();
+      tc_before_sync();
+      __syncthreads();
+      if (t == 0) {
+        tc_after_sync();
+        if (layer == 0) issue_layer(smem, tmem, OFF_X, OFF_W1, K1, 64, bar);
+        else if (layer == 1) issue_layer(smem, tmem, OFF_H, OFF_W2, 64, 64, bar);
+        else issue_layer(smem, tmem, OFF_H, OFF_W3, 64, N3, bar);
+      }
+      const bool ok = bar_wait(bar, phase);
+      phase ^= 1u;
+      if (__syncthreads_or(!ok)) {
+        failed = true;
+        break;
+      }
+      tc_after_sync();
+      float a[32];
+      tmem_ld32(trow, a);
+#pragma unroll
+      for (int i = 0; i < 32; ++i) v[i] = a[i];
+      if (layer < 2) {
+        tmem_ld32(trow + 32, a);
+#pragma unroll
+        for (int i = 0; i < 32; ++i) v[32 + i] = a[i];
+        const float* bias = sb + 64 * layer;
+#pragma unroll
+        for (int i = 0; i < 64; ++i) v[i] = gelu_fast(v[i] + bias[i]);
+#pragma unroll
+        for (int ch = 0; ch < 8; ++ch) store_chunk(smem + OFF_H, t, ch, TILE, v + 8 * ch);
+      }
+    }
+    if (failed) break;
+    // ---- output row
+    if (MODE == 0) {
+      if (scale != 0.0f) {
+#pragma unroll
+        for (int i = 0; i < D::NR; ++i)
+          if (g[i] >= 0) atomicAdd(z + g[i], T(scale * (v[i] + sb[128 + i]) * __ldg(winv + g[i])));
+      }
+    } else if (live) {
+#pragma unroll
+      for (int j = 0; j < D::NOUT; ++j) zout[c * D::NOUT + j] = v[j] + sb[128 + j];
+    }
+    // the next tile's layer-1 MMA overwrites the accumulator read above
+    tc_before_sync();
+  }
+  if (failed && t == 0) {
+    atomicOr(status, 1);
+    bar_wait(bar, phase ^ 1u);  // the MMAs of the timed-out commit
+  }
+  tc_before_sync();
+  __syncthreads();
+  tc_after_sync();
+  if (warp == 0)
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(uint32_t(TMEM_COLS))
+                 : "memory");
+}
+
+}  // namespace sfem

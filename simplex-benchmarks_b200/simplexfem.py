@@ -133,6 +133,9 @@ _PROTOS = [
     ("fem_mlp_gradient", C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_int32, C.c_void_p,
                                    C.POINTER(C.c_double), C.c_void_p]),
     ("fem_mlp_forward", C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_int32, C.c_void_p]),
+    ("fem_mlp_forward_tc", C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_int32, C.c_void_p]),
+    ("fem_mlp_set_tensor_cores", C.c_int, [C.c_void_p, C.c_int32]),
+    ("fem_mlp_status", C.c_int, [C.c_void_p, C.POINTER(C.c_int32)]),
     ("fem_mlp_save", C.c_int, [C.c_void_p, C.c_char_p]),
     ("fem_mlp_load", C.c_int, [C.c_char_p, C.POINTER(C.c_void_p)]),
     ("fem_mg_set_learned_smoother", C.c_int, [C.c_void_p, C.c_void_p, C.c_int32]),
@@ -531,11 +534,24 @@ class MLP:
                                      _stream_ptr(stream)))
         return g, loss.value
 
-    def forward(self, X, stream=None):
+    def forward(self, X, stream=None, tensor_cores=False):
+        """O [n][20] = MLP(X [n][29]) (device float32 tensors); tensor_cores
+        selects the tcgen05 kernel (BF16 activations)."""
         import torch
         O = torch.zeros((X.shape[0], 20), dtype=torch.float32, device="cuda")
-        check(lib().fem_mlp_forward(self.handle, _ptr(X), _ptr(O), X.shape[0], _stream_ptr(stream)))
+        fn = lib().fem_mlp_forward_tc if tensor_cores else lib().fem_mlp_forward
+        check(fn(self.handle, _ptr(X), _ptr(O), X.shape[0], _stream_ptr(stream)))
         return O
+
+    def set_tensor_cores(self, on):
+        """Smooth on the tensor cores (default) or on the CUDA cores."""
+        check(lib().fem_mlp_set_tensor_cores(self.handle, int(bool(on))))
+
+    def timed_out(self):
+        """True if a tensor-core launch gave up on a bounded wait since the last call."""
+        v = C.c_int32()
+        check(lib().fem_mlp_status(self.handle, C.byref(v)))
+        return bool(v.value)
 
     def __del__(self):
         if getattr(self, "handle", None) and _lib is not None:

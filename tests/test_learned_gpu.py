@@ -38,6 +38,23 @@ def test_mlp_forward_matches_oracle(cuda):
     assert np.abs(O - ref).max() <= 1e-4 * max(1.0, np.abs(ref).max())
 
 
+@pytest.mark.parametrize("n", [50, 128, 1000])
+def test_mlp_tensor_core_forward_matches_oracle(cuda, n):
+    """tcgen05 forward (BF16 operands, FP32 tensor-memory accumulators, hardware
+    tanh in the GELU) vs the FP64 oracle with BF16-rounded inputs and
+    activations.  Tolerance: rel l2 <= 1e-2 and max error <= 3e-2 of the output
+    scale (a BF16 ulp is 2^-8 relative; the hardware tanh adds ~2^-11)."""
+    import torch
+    mlp = sf.MLP(seed=7)
+    X, _ = _data(n, 4)
+    O = mlp.forward(torch.tensor(X, device="cuda"), tensor_cores=True).cpu().numpy()
+    assert not mlp.timed_out()
+    ref, _ = mlp_oracle.forward(mlp.weights(), X, bf16_activations=True)
+    scale = max(1.0, np.abs(ref).max())
+    assert np.linalg.norm(O - ref) <= 1e-2 * np.linalg.norm(ref)
+    assert np.abs(O - ref).max() <= 3e-2 * scale
+
+
 def test_training_fits_a_linear_map(cuda):
     """Adam on the GPU kernels drives the loss of a learnable target down."""
     import torch
