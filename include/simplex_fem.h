@@ -196,7 +196,10 @@ typedef struct fem_mg_params {
   double eig_safety;        /* lambda_max = safety * estimate (1.2) */
   int32_t coarse_n;         /* hexes per direction on the coarsest level (4) */
   int32_t use_graph;        /* capture the V-cycle as a CUDA graph (1) */
-  int32_t reserved[4];
+  int32_t c_transfer;       /* FEM_DG fine operators: 0 = DG P_p .. P_1 then CG P_1 (phc),
+                               1 = CG P_p right below DG P_p, then the CG ladder of `order`
+                               (cph / chp; DG/cells_batched/application_phc.cc:3396-3652) */
+  int32_t reserved[3];
 } fem_mg_params;
 int fem_mg_params_default(fem_mg_params* p);
 int fem_mg_create(fem_op* fine, const fem_mg_params* p, fem_mg** out);
@@ -204,6 +207,8 @@ int fem_mg_destroy(fem_mg* mg);
 int fem_mg_n_levels(const fem_mg* mg, int32_t* n);
 int fem_mg_level_info(const fem_mg* mg, int32_t level, uint64_t* m, int32_t* degree, int32_t* hexes,
                       double* lambda_max);
+/* FEM_CG or FEM_DG: the kind of a level's operator (DG hierarchies have both) */
+int fem_mg_level_kind(const fem_mg* mg, int32_t level, int32_t* kind);
 /* PreconditionMG::vmult: dst = V(src), FP64 vectors of the fine operator */
 int fem_mg_vcycle(fem_mg* mg, double* dst, const double* src, void* stream);
 /* MG hooks on level-precision vectors of length level m: mg::Matrix::vmult,

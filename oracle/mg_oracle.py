@@ -14,7 +14,10 @@ application_hp.cc:1735-2008) and SolverCG (:1949-1980):
     lambda_min = lambda_max / smoothing_range;
   - a direct coarse solve (the reference's AMG on a 125-DoF coarse grid
     reduces to an exact solve for the purpose of counting iterations);
-  - PCG stopping at ||r|| <= rtol ||b||.
+  - PCG stopping at ||r|| <= rtol ||b||;
+  - DG hierarchies (DGMGOracle): DG P_p .. P_pc by cell-local embeddings, a
+    c-transfer from CG P_pc, then the CG ladder
+    (DG/cells_batched/application_phc.cc:3396-3652).
 Meshes must be unjittered (nested Kuhn refinement).  Parity status: unpinned
 against the reference (deal.II and Trilinos are absent); checked against the
 GPU solver's iteration counts.
@@ -188,6 +191,89 @@ class MGOracle:
         xc = self.vcycle(self.P[l].T @ r, l - 1)
         x = x + self.P[l] @ xc
         return self._smooth(L, x, b, False)
+
+
+class DGLevel:
+    """DG level (FE_SimplexDGP, SIPG) assembled by probing the oracle's vmult.
+    A DG row of cell c couples only to cell c and its face neighbours, so the
+    cells are given a distance-2 colouring and one probe per (colour, local
+    DoF) recovers all columns of that colour; small meshes only."""
+
+    def __init__(self, mesh, p):
+        o = orc.for_mesh(mesh, p, orc.DG)
+        self.mesh, self.p, self.n = mesh, p, o.n
+        C = mesh.n_cells
+        K = self.n // C
+        nb, _ = mesh.neighbors()
+        adj = [set(int(v) for v in nb[c] if v >= 0) for c in range(C)]
+        color = np.full(C, -1)
+        for c in range(C):
+            near = set(adj[c])
+            for a in adj[c]:
+                near |= adj[a]
+            used = {color[a] for a in near if color[a] >= 0}
+            color[c] = next(k for k in range(len(used) + 1) if k not in used)
+        rows, cols, vals = [], [], []
+        for k in range(color.max() + 1):
+            cells = np.nonzero(color == k)[0]
+            for i in range(K):
+                e = np.zeros(self.n)
+                e[cells * K + i] = 1.0
+                y = o.vmult(e)
+                for c in cells:
+                    for a in [c] + sorted(adj[c]):
+                        blk = y[a * K:(a + 1) * K]
+                        nz = np.nonzero(blk)[0]
+                        rows.append(a * K + nz)
+                        cols.append(np.full(nz.size, c * K + i))
+                        vals.append(blk[nz])
+        self.A = sp.coo_matrix((np.concatenate(vals), (np.concatenate(rows), np.concatenate(cols))),
+                               shape=(self.n, self.n)).tocsr()
+        self.cm = np.zeros(self.n, np.uint8)
+        d = self.A.diagonal()
+        self.invd = np.where(np.abs(d) > 1e-10, 1.0 / d, 1.0)
+
+
+def embedding(p):
+    """Nodal interpolation of P_{p-1} at the P_p nodes, [K_p][K_{p-1}]."""
+    L = lattice_nodes(p)
+    return np.array([orc.basis(p - 1, lam[1:])[0] for lam in L])
+
+
+class DGMGOracle(MGOracle):
+    """DG multigrid of DG/cells_batched/application_phc.cc:3396-3652: DG levels
+    P_p .. P_pc on the fine mesh (cell-local embeddings), a c-transfer from CG
+    P_pc on the same mesh (continuous nodal values copied into every cell,
+    constrained nodes as 0), then the CG ladder of MGOracle.  pc = 1
+    (c_transfer 0, phc) or p (c_transfer 1, cph / chp).  The CG levels keep the
+    strong homogeneous Dirichlet constraints of the CG operator."""
+
+    def __init__(self, make_mesh, n, p, c_transfer=0, order="ph", coarse_n=4, degree=3, smoothing_range=20.0,
+                 eig_iterations=10, eig_safety=1.2, seed=0):
+        pc = 1 if c_transfer == 0 else p
+        super().__init__(make_mesh, n, pc, order=order, coarse_n=coarse_n, degree=degree,
+                         smoothing_range=smoothing_range, eig_iterations=eig_iterations, eig_safety=eig_safety,
+                         seed=seed)
+        mesh = make_mesh(n)
+        cgtop = self.levels[-1]
+        rng = np.random.default_rng(seed + 1)
+        for q in range(pc, p + 1):
+            L = DGLevel(mesh, q)
+            C = mesh.n_cells
+            if q == pc:
+                K = cgtop.cd.shape[1]
+                free = ~cgtop.cm.astype(bool)
+                r = np.arange(C * K)
+                g = cgtop.cd.reshape(-1)
+                ok = free[g]
+                P = sp.coo_matrix((np.ones(ok.sum()), (r[ok], g[ok])), shape=(L.n, cgtop.n)).tocsr()
+            else:
+                E = embedding(q)
+                P = sp.kron(sp.identity(C, format="csr"), sp.csr_matrix(E)).tocsr()
+            L.lmax = eig_safety * self._lanczos_max(L, eig_iterations, rng)
+            L.lmin = L.lmax / smoothing_range
+            self.levels.append(L)
+            self.P.append(P)
 
 
 def pcg(A, b, precond, rtol, maxit):

@@ -80,6 +80,7 @@ int fem_mg_params_default(fem_mg_params* p) {
     p->eig_safety = d.eig_safety;
     p->coarse_n = d.coarse_n;
     p->use_graph = d.use_graph;
+    p->c_transfer = d.c_transfer;
   });
 }
 
@@ -97,6 +98,7 @@ int fem_mg_create(fem_op* fine, const fem_mg_params* p, fem_mg** out) {
       prm.eig_safety = p->eig_safety;
       prm.coarse_n = p->coarse_n;
       prm.use_graph = p->use_graph;
+      prm.c_transfer = p->c_transfer;
     }
     SFEM_REQUIRE(prm.order == FEM_MG_PH || prm.order == FEM_MG_HP, FEM_ERR_ARG, "mg: order must be PH or HP");
     SFEM_REQUIRE(prm.eig_iterations >= 1 && prm.smoothing_range > 1 && prm.eig_safety >= 1, FEM_ERR_ARG,
@@ -128,6 +130,15 @@ int fem_mg_level_info(const fem_mg* mg, int32_t level, uint64_t* m, int32_t* deg
     if (degree) *degree = mg->mg->level_degree(level);
     if (hexes) *hexes = mg->mg->level_hexes(level);
     if (lambda_max) *lambda_max = mg->mg->level_lambda_max(level);
+  });
+}
+
+int fem_mg_level_kind(const fem_mg* mg, int32_t level, int32_t* kind) {
+  return guarded([&] {
+    SFEM_REQUIRE_PTR(mg);
+    SFEM_REQUIRE_PTR(kind);
+    SFEM_REQUIRE(level >= 0 && level < mg->mg->n_levels(), FEM_ERR_ARG, "mg: level out of range");
+    *kind = mg->mg->level_operator(level).cfg.kind;
   });
 }
 

@@ -97,6 +97,63 @@ __global__ void transfer_restrict_add(int64_t nf, int Kf, int Kc, const int32_t*
   }
 }
 
+// DG p-transfer on one mesh: cell-local embedding P_{p-1} -> P_p, no sharing
+// (DG/cells_batched/application_phc.cc:3396-3475 builds the same two-level
+// transfer with MGTwoLevelTransfer on FE_SimplexDGP).  Layout [cell][K].
+template <typename T>
+__global__ void dg_p_prolongate_add(int64_t n, int Kf, int Kc, const double* __restrict__ emb,
+                                    const T* __restrict__ xc, T* __restrict__ xf) {
+  const int64_t c = blockIdx.x * int64_t(blockDim.x) + threadIdx.x;
+  if (c >= n) return;
+  double xl[20];
+  for (int j = 0; j < Kc; ++j) xl[j] = double(xc[c * Kc + j]);
+  for (int i = 0; i < Kf; ++i) {
+    double acc = 0.0;
+    for (int j = 0; j < Kc; ++j) acc += emb[i * Kc + j] * xl[j];
+    xf[c * Kf + i] += T(acc);
+  }
+}
+
+template <typename T>
+__global__ void dg_p_restrict_add(int64_t n, int Kf, int Kc, const double* __restrict__ emb,
+                                  const T* __restrict__ xf, T* __restrict__ xc) {
+  const int64_t c = blockIdx.x * int64_t(blockDim.x) + threadIdx.x;
+  if (c >= n) return;
+  double rl[20];
+  for (int i = 0; i < Kf; ++i) rl[i] = double(xf[c * Kf + i]);
+  for (int j = 0; j < Kc; ++j) {
+    double acc = 0.0;
+    for (int i = 0; i < Kf; ++i) acc += emb[i * Kc + j] * rl[i];
+    xc[c * Kc + j] += T(acc);
+  }
+}
+
+// c-transfer between CG P_q and DG P_q on the same mesh
+// (DG/cells_batched/application_phc.cc:3476-3552): prolongation copies the
+// continuous nodal values into every cell (0 at constrained nodes),
+// restriction sums the cells' values back (its transpose).
+template <typename T>
+__global__ void c_prolongate_add(int64_t n, int K, const int32_t* __restrict__ cdofs, const T* __restrict__ xcg,
+                                 T* __restrict__ xdg) {
+  const int64_t c = blockIdx.x * int64_t(blockDim.x) + threadIdx.x;
+  if (c >= n) return;
+  for (int i = 0; i < K; ++i) {
+    const int32_t g = cdofs[i * n + c];
+    if (g >= 0) xdg[c * K + i] += xcg[g];
+  }
+}
+
+template <typename T>
+__global__ void c_restrict_add(int64_t n, int K, const int32_t* __restrict__ cdofs, const T* __restrict__ xdg,
+                               T* __restrict__ xcg) {
+  const int64_t c = blockIdx.x * int64_t(blockDim.x) + threadIdx.x;
+  if (c >= n) return;
+  for (int i = 0; i < K; ++i) {
+    const int32_t g = cdofs[i * n + c];
+    if (g >= 0) atomicAdd(xcg + g, xdg[c * K + i]);
+  }
+}
+
 // basis of P_p at reference point xi
 void eval_basis(int p, const double xi[3], double* out) {
   auto ev = [&](auto tag) {
@@ -315,6 +372,9 @@ class MultigridImpl final : public Multigrid {
  public:
   struct Level {
     const Mesh* mesh = nullptr;
+    int kind = FEM_CG;
+    // transfer from level-1: cell-based CG p/h, DG embedding, or CG -> DG
+    enum { T_NONE, T_CG, T_DGP, T_C } ttype = T_NONE;
     std::unique_ptr<Operator> op;
     DevBuf<T> inv_diag, x, b, r, t, d;
     double lmax = 0, lmin = 0;
@@ -343,7 +403,9 @@ class MultigridImpl final : public Multigrid {
 
   MultigridImpl(const Operator& fine, const MGParams& prm) {
     params = prm;
-    SFEM_REQUIRE(fine.cfg.kind == FEM_CG && fine.mesh, FEM_ERR_ARG, "multigrid: fine operator must be CG");
+    SFEM_REQUIRE((fine.cfg.kind == FEM_CG || fine.cfg.kind == FEM_DG) && fine.mesh, FEM_ERR_ARG,
+                 "multigrid: fine operator must be CG or DG (one component)");
+    SFEM_REQUIRE(prm.c_transfer == 0 || prm.c_transfer == 1, FEM_ERR_ARG, "multigrid: c_transfer must be 0 or 1");
     SFEM_REQUIRE(prm.smoother_degree >= 1 && prm.smoother_degree <= 32, FEM_ERR_ARG, "multigrid: smoother degree");
     const Mesh& mf = *fine.mesh;
     fine_m_ = fine.m;
@@ -368,24 +430,35 @@ class MultigridImpl final : public Multigrid {
       mesh_of[k] = meshes_.back().get();
     }
     const int p = fine.cfg.degree;
-    std::vector<std::pair<const Mesh*, int>> seq;  // coarse -> fine
+    const bool dg = fine.cfg.kind == FEM_DG;
+    // CG ladder up to degree pc on the fine mesh, then (DG) DG levels pc .. p
+    const int pc = dg && prm.c_transfer == 0 ? 1 : p;
+    struct Spec {
+      const Mesh* mesh;
+      int degree, kind;
+    };
+    std::vector<Spec> seq;  // coarse -> fine
     if (prm.order == MG_ORDER_PH) {
-      for (int k = H; k >= 0; --k) seq.push_back({mesh_of[k], 1});
-      for (int q = 2; q <= p; ++q) seq.push_back({&mf, q});
+      for (int k = H; k >= 0; --k) seq.push_back({mesh_of[k], 1, FEM_CG});
+      for (int q = 2; q <= pc; ++q) seq.push_back({&mf, q, FEM_CG});
     } else {
-      for (int q = 1; q <= p; ++q) seq.push_back({mesh_of[H], q});
-      for (int k = H - 1; k >= 0; --k) seq.push_back({mesh_of[k], p});
+      for (int q = 1; q <= pc; ++q) seq.push_back({mesh_of[H], q, FEM_CG});
+      for (int k = H - 1; k >= 0; --k) seq.push_back({mesh_of[k], pc, FEM_CG});
     }
+    if (dg)
+      for (int q = pc; q <= p; ++q) seq.push_back({&mf, q, FEM_DG});
     levels_.resize(seq.size());
     OpConfig cfg;
-    cfg.kind = FEM_CG;
     cfg.precision = std::is_same<T, double>::value ? FEM_FP64 : FEM_FP32;
+    cfg.penalty = fine.cfg.penalty;
     for (size_t l = 0; l < seq.size(); ++l) {
       Level& L = levels_[l];
-      L.mesh = seq[l].first;
-      L.degree = seq[l].second;
+      L.mesh = seq[l].mesh;
+      L.degree = seq[l].degree;
+      L.kind = seq[l].kind;
       L.hexes = L.mesh->desc.n[0];
       cfg.degree = L.degree;
+      cfg.kind = L.kind;
       L.op = make_operator(*L.mesh, cfg);
       const int64_t m = L.op->m;
       L.inv_diag.alloc(m);
@@ -401,6 +474,25 @@ class MultigridImpl final : public Multigrid {
     for (size_t l = 1; l < levels_.size(); ++l) {
       Level& F = levels_[l];
       const Level& Cl = levels_[l - 1];
+      if (F.kind == FEM_DG && Cl.kind == FEM_DG) {
+        F.ttype = Level::T_DGP;
+        F.Kf = k_of_deg(F.degree);
+        F.Kc = k_of_deg(Cl.degree);
+        std::vector<double> emb(size_t(F.Kf) * F.Kc);
+        for (int i = 0; i < F.Kf; ++i)
+          for (int j = 0; j < F.Kc; ++j)
+            emb[i * F.Kc + j] = F.degree == 2 ? ref::Tables<2>::EMB[i][j] : ref::Tables<3>::EMB[i][j];
+        F.mats.upload(emb);
+        continue;
+      }
+      if (F.kind == FEM_DG) {
+        SFEM_REQUIRE(Cl.kind == FEM_CG && Cl.degree == F.degree && Cl.mesh == F.mesh, FEM_ERR_INTERNAL,
+                     "multigrid: c-transfer needs CG and DG of one degree on one mesh");
+        F.ttype = Level::T_C;
+        F.Kf = F.Kc = k_of_deg(F.degree);
+        continue;
+      }
+      F.ttype = Level::T_CG;
       TransferHost th = F.mesh == Cl.mesh ? make_p_transfer(*F.op) : make_h_transfer(*F.op, *Cl.op);
       F.Kf = th.Kf;
       F.Kc = th.Kc;
@@ -431,7 +523,8 @@ class MultigridImpl final : public Multigrid {
   void set_learned(LearnedSmoother* s, bool fallback) override {
     if (s) {
       const Level& top = levels_.back();
-      SFEM_REQUIRE(top.degree == 3, FEM_ERR_ARG, "learned smoother: the finest level must be P3");
+      SFEM_REQUIRE(top.degree == 3 && top.kind == FEM_CG, FEM_ERR_ARG,
+                   "learned smoother: the finest level must be CG P3");
     }
     learned_ = s;
     use_learned_ = s != nullptr;
@@ -470,7 +563,8 @@ class MultigridImpl final : public Multigrid {
       st ^= st << 13;
       st ^= st >> 7;
       st ^= st << 17;
-      h[i] = L.op->constrained[i] ? T(0) : T(double(st >> 11) * (2.0 / 9007199254740992.0) - 1.0);
+      const bool fixed = !L.op->constrained.empty() && L.op->constrained[i];
+      h[i] = fixed ? T(0) : T(double(st >> 11) * (2.0 / 9007199254740992.0) - 1.0);
     }
     L.r.upload(h);  // r = b (x = 0)
     const unsigned g = grid_for(m);
@@ -594,7 +688,20 @@ class MultigridImpl final : public Multigrid {
     Level& F = levels_.at(l);
     SFEM_REQUIRE(l > 0, FEM_ERR_ARG, "prolongate: level must be >= 1");
     const Level& Cl = levels_[l - 1];
-    transfer_prolongate_add<T><<<unsigned((F.op->n_cells + 127) / 128), 128, 0, s>>>(
+    const unsigned grid = unsigned((F.op->n_cells + 127) / 128);
+    if (F.ttype == Level::T_DGP) {
+      dg_p_prolongate_add<T><<<grid, 128, 0, s>>>(F.op->n_cells, F.Kf, F.Kc, F.mats.p, static_cast<const T*>(src),
+                                                  static_cast<T*>(dst));
+      SFEM_CUDA(cudaGetLastError());
+      return;
+    }
+    if (F.ttype == Level::T_C) {
+      c_prolongate_add<T><<<grid, 128, 0, s>>>(F.op->n_cells, F.Kf, Cl.op->device_dof_table(),
+                                               static_cast<const T*>(src), static_cast<T*>(dst));
+      SFEM_CUDA(cudaGetLastError());
+      return;
+    }
+    transfer_prolongate_add<T><<<grid, 128, 0, s>>>(
         F.op->n_cells, F.Kf, F.Kc, F.parent.p, F.mat_id.p, F.owner.p, F.mats.p, F.op->device_dof_table(),
         Cl.op->device_dof_table(), Cl.op->n_cells, static_cast<const T*>(src), static_cast<T*>(dst));
     SFEM_CUDA(cudaGetLastError());
@@ -604,7 +711,20 @@ class MultigridImpl final : public Multigrid {
     Level& F = levels_.at(l);
     SFEM_REQUIRE(l > 0, FEM_ERR_ARG, "restrict: level must be >= 1");
     const Level& Cl = levels_[l - 1];
-    transfer_restrict_add<T><<<unsigned((F.op->n_cells + 127) / 128), 128, 0, s>>>(
+    const unsigned grid = unsigned((F.op->n_cells + 127) / 128);
+    if (F.ttype == Level::T_DGP) {
+      dg_p_restrict_add<T><<<grid, 128, 0, s>>>(F.op->n_cells, F.Kf, F.Kc, F.mats.p, static_cast<const T*>(src),
+                                                static_cast<T*>(dst));
+      SFEM_CUDA(cudaGetLastError());
+      return;
+    }
+    if (F.ttype == Level::T_C) {
+      c_restrict_add<T><<<grid, 128, 0, s>>>(F.op->n_cells, F.Kf, Cl.op->device_dof_table(),
+                                             static_cast<const T*>(src), static_cast<T*>(dst));
+      SFEM_CUDA(cudaGetLastError());
+      return;
+    }
+    transfer_restrict_add<T><<<grid, 128, 0, s>>>(
         F.op->n_cells, F.Kf, F.Kc, F.parent.p, F.mat_id.p, F.owner.p, F.mats.p, F.op->device_dof_table(),
         Cl.op->device_dof_table(), Cl.op->n_cells, static_cast<const T*>(src), static_cast<T*>(dst));
     SFEM_CUDA(cudaGetLastError());

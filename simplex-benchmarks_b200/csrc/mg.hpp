@@ -1,7 +1,8 @@
-// Hybrid (p/h) multigrid V-cycle and the preconditioned CG solver.
+// Hybrid (p/h/c) multigrid V-cycle and the preconditioned CG solver.
 //
 // Replaces MultigridPreconditioner (CG/cells_batched/application_ph.cc:
-// 1754-2023, h-then-p order application_hp.cc:1735-2008) and SolverCG +
+// 1754-2023, h-then-p order application_hp.cc:1735-2008; DG p/c/h orders
+// DG/cells_batched/application_phc.cc:3396-3652) and SolverCG +
 // PreconditionMG (application_ph.cc:1949-1980).
 #pragma once
 #include <cuda_runtime.h>
@@ -24,6 +25,11 @@ struct MGParams {
   double eig_safety = 1.2;      // lambda_max = safety * estimate
   int coarse_n = 4;             // hexes per direction of the coarsest mesh
   int use_graph = 1;            // capture the V-cycle in a CUDA graph
+  // DG fine operators: degree at which the DG levels hand over to CG levels
+  // on the same mesh (c-transfer).  0: DG P_p .. P_1, then CG P_1 (the
+  // reference's phc order); 1: CG P_p right below DG P_p, then the CG p/h
+  // ladder of `order` (cph with FEM_MG_PH, chp with FEM_MG_HP).
+  int c_transfer = 0;
 };
 
 class Multigrid {

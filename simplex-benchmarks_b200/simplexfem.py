@@ -48,7 +48,8 @@ class RhsDesc(C.Structure):
 class MGParams(C.Structure):
     _fields_ = [("order", C.c_int32), ("precision", C.c_int32), ("smoother_degree", C.c_int32),
                 ("eig_iterations", C.c_int32), ("smoothing_range", C.c_double), ("eig_safety", C.c_double),
-                ("coarse_n", C.c_int32), ("use_graph", C.c_int32), ("reserved", C.c_int32 * 4)]
+                ("coarse_n", C.c_int32), ("use_graph", C.c_int32), ("c_transfer", C.c_int32),
+                ("reserved", C.c_int32 * 3)]
 
 
 class SolveInfo(C.Structure):
@@ -111,6 +112,7 @@ _PROTOS = [
     ("fem_mg_n_levels", C.c_int, [C.c_void_p, C.POINTER(C.c_int32)]),
     ("fem_mg_level_info", C.c_int, [C.c_void_p, C.c_int32, C.POINTER(C.c_uint64), C.POINTER(C.c_int32),
                                     C.POINTER(C.c_int32), C.POINTER(C.c_double)]),
+    ("fem_mg_level_kind", C.c_int, [C.c_void_p, C.c_int32, C.POINTER(C.c_int32)]),
     ("fem_mg_vcycle", C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]),
     ("fem_mg_level_vmult", C.c_int, [C.c_void_p, C.c_int32, C.c_void_p, C.c_void_p, C.c_void_p]),
     ("fem_mg_smooth", C.c_int, [C.c_void_p, C.c_int32, C.c_void_p, C.c_void_p, C.c_int32, C.c_void_p]),
@@ -375,10 +377,12 @@ def interpolate(op, desc, dst=None, stream=None):
 
 
 class Multigrid:
-    """Hybrid p/h multigrid on a CG operator (fem_mg); MultigridPreconditioner's shape."""
+    """Hybrid p/h/c multigrid on a CG or DG operator (fem_mg); MultigridPreconditioner's shape.
+    DG: c_transfer=0 coarsens DG P_p .. P_1 then hands over to CG P_1 (phc);
+    c_transfer=1 hands over at P_p (cph with FEM_MG_PH, chp with FEM_MG_HP)."""
 
     def __init__(self, fine_op, order=FEM_MG_PH, precision="fp32", smoother_degree=3, smoothing_range=20.0,
-                 eig_iterations=10, eig_safety=1.2, coarse_n=4, use_graph=True):
+                 eig_iterations=10, eig_safety=1.2, coarse_n=4, use_graph=True, c_transfer=0):
         p = MGParams()
         check(lib().fem_mg_params_default(C.byref(p)))
         p.order = order
@@ -389,6 +393,7 @@ class Multigrid:
         p.eig_safety = eig_safety
         p.coarse_n = coarse_n
         p.use_graph = int(bool(use_graph))
+        p.c_transfer = c_transfer
         h = C.c_void_p()
         check(lib().fem_mg_create(fine_op.handle, C.byref(p), C.byref(h)))
         self.handle = h
@@ -401,7 +406,10 @@ class Multigrid:
     def level_info(self, level):
         m, d, hx, lm = C.c_uint64(), C.c_int32(), C.c_int32(), C.c_double()
         check(lib().fem_mg_level_info(self.handle, level, C.byref(m), C.byref(d), C.byref(hx), C.byref(lm)))
-        return {"m": m.value, "degree": d.value, "hexes": hx.value, "lambda_max": lm.value}
+        kd = C.c_int32()
+        check(lib().fem_mg_level_kind(self.handle, level, C.byref(kd)))
+        return {"m": m.value, "degree": d.value, "hexes": hx.value, "lambda_max": lm.value,
+                "kind": {FEM_CG: "cg", FEM_DG: "dg"}.get(kd.value, kd.value)}
 
     def level_vector(self, level):
         import torch

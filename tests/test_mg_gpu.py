@@ -174,3 +174,32 @@ def test_config3_full_size(cuda):
         assert float(torch.linalg.norm(b - r) / torch.linalg.norm(b)) <= 1.01e-8
         del mg
     assert abs(its["fp32"] - its["fp64"]) <= 1 and its["fp32"] <= 12, its
+
+
+@pytest.mark.parametrize("p,c_transfer,order", [(2, 0, sf.FEM_MG_PH), (3, 0, sf.FEM_MG_PH),
+                                                (3, 1, sf.FEM_MG_PH), (3, 1, sf.FEM_MG_HP)])
+def test_dg_multigrid_iterations_match_oracle(cuda, p, c_transfer, order):
+    """DG (SIPG) P_p solved by CG with the p/c/h multigrid (phc: DG P_p .. P_1,
+    CG P_1, h-levels; cph/chp: CG P_p right below DG P_p): iteration count to
+    1e-8 within +-1 of the CPU oracle's multigrid on the same problem."""
+    import torch
+    n = 4
+    mesh = sf.Mesh(n)
+    op = sf.Operator(mesh, p, "dg")
+    mg = sf.Multigrid(op, order=order, precision="fp64", coarse_n=2, c_transfer=c_transfer)
+    kinds = [mg.level_info(l)["kind"] for l in range(mg.n_levels)]
+    assert kinds[-1] == "dg" and kinds[0] == "cg"
+    assert kinds.count("dg") == (p if c_transfer == 0 else 1)
+    rng = np.random.default_rng(5)
+    bh = rng.uniform(-1, 1, op.m())
+    b = torch.tensor(bh, device="cuda")
+    x = op.initialize_dof_vector()
+    res = sf.SolverCG(op, mg).solve(x, b, rtol=1e-8, max_iterations=100)
+    assert res["status"] == sf.FEM_OK, res
+    M = mgo.DGMGOracle(lambda k: sf.Mesh(k), n, p, c_transfer=c_transfer,
+                       order="ph" if order == sf.FEM_MG_PH else "hp", coarse_n=2)
+    top = M.levels[-1]
+    _, its = mgo.pcg(lambda v: top.A @ v, bh, M.vcycle, 1e-8, 100)
+    assert abs(res["iterations"] - its) <= 1, (res["iterations"], its)
+    xs = x.cpu().numpy()
+    assert np.linalg.norm(top.A @ xs - bh) <= 1.1e-8 * np.linalg.norm(bh)

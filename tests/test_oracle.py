@@ -134,3 +134,22 @@ def test_mg_oracle_converges_mesh_independently(p, order):
         assert np.linalg.norm(b - top.A @ x) <= 1e-8 * np.linalg.norm(b)
         its.append(it)
     assert max(its) <= 12 and abs(its[0] - its[1]) <= 2, its
+
+
+def test_dg_mg_oracle_levels_and_convergence():
+    """The probed DG level matrix equals the oracle's DG vmult and is symmetric;
+    the DG p/c/h multigrid oracle (phc) converges far faster than Jacobi."""
+    import mg_oracle as mgo
+    mesh = sf.Mesh(3, jitter=0.1, seed=1)
+    L = mgo.DGLevel(mesh, 2)
+    o = orc.for_mesh(mesh, 2, orc.DG)
+    x = np.random.default_rng(0).uniform(-1, 1, L.n)
+    assert np.linalg.norm(L.A @ x - o.vmult(x)) <= 1e-13 * np.linalg.norm(o.vmult(x))
+    assert abs(L.A - L.A.T).max() <= 1e-13 * abs(L.A).max()
+    M = mgo.DGMGOracle(lambda k: sf.Mesh(k), 4, 2, c_transfer=0, coarse_n=2)
+    assert [type(l).__name__ for l in M.levels] == ["Level", "Level", "DGLevel", "DGLevel"]
+    top = M.levels[-1]
+    b = np.random.default_rng(5).uniform(-1, 1, top.n)
+    _, its_mg = mgo.pcg(lambda v: top.A @ v, b, M.vcycle, 1e-8, 100)
+    _, its_j = mgo.pcg(lambda v: top.A @ v, b, lambda r: top.invd * r, 1e-8, 2000)
+    assert its_mg < 30 and its_mg * 5 < its_j, (its_mg, its_j)
