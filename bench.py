@@ -34,13 +34,16 @@ for p in (os.path.join(ROOT, "simplex-benchmarks_b200"), os.path.join(ROOT, "ora
 N_HEX, DEGREE, JITTER = 32, 3, 0.1
 METRIC = "vmult DoF/s (FP64 vs mixed); Poisson solve time to 1e-8 (MG vs learned)"
 WORKLOAD = "DG SIPG Poisson vmult, P3 on 32^3 x 6 Kuhn tets (196,608 cells, 3,932,160 DoFs), jitter 0.1h"
+# dram__bytes_read.sum + dram__bytes_write.sum of one dg_apply_kernel<3,1,false,64,double>
+# launch on this workload (ncu --set full capture, 89.25 MB read + 14.0 MB written)
+APPLY_TRAFFIC_BYTES = 103.3e6
 
 
 def parse():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=20)
-    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--steps", type=int, default=500)
+    ap.add_argument("--warmup", type=int, default=10)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-solve", action="store_true", help="skip the multigrid solve measurement")
@@ -57,11 +60,36 @@ class ClockSampler:
          "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
          "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
 
-    def __init__(self, gpu):
+    def __init__(self, gpu, interval=0.02):
         self.gpu = gpu
+        self.interval = interval
         self.proc = None
+        self.samples = []  # (sm_mhz, max_mhz, reasons)
+        self.nvml = None
+
+    def _poll(self):
+        import pynvml as nv
+        h = nv.nvmlDeviceGetHandleByIndex(self.gpu)
+        mx = nv.nvmlDeviceGetMaxClockInfo(h, nv.NVML_CLOCK_SM)
+        bits = {"hw_slowdown": 0x8, "sw_thermal_slowdown": 0x20, "hw_thermal_slowdown": 0x40, "sw_power_cap": 0x4}
+        while not self.stop.is_set():
+            sm = nv.nvmlDeviceGetClockInfo(h, nv.NVML_CLOCK_SM)
+            r = nv.nvmlDeviceGetCurrentClocksEventReasons(h)
+            self.samples.append((float(sm), float(mx), [k for k, v in bits.items() if r & v]))
+            time.sleep(self.interval)
 
     def __enter__(self):
+        try:
+            import threading
+            import pynvml as nv
+            nv.nvmlInit()
+            self.nvml = nv
+            self.stop = threading.Event()
+            self.thread = threading.Thread(target=self._poll, daemon=True)
+            self.thread.start()
+            return self
+        except Exception:
+            self.nvml = None
         try:
             self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.gpu), f"--query-gpu={self.Q}",
                                           "--format=csv,noheader,nounits", "-lms", "200"],
@@ -72,6 +100,11 @@ class ClockSampler:
 
     def __exit__(self, *a):
         self.out = ""
+        if self.nvml:
+            time.sleep(2 * self.interval)
+            self.stop.set()
+            self.thread.join(timeout=5)
+            return
         if self.proc:
             time.sleep(0.25)
             self.proc.terminate()
@@ -83,6 +116,10 @@ class ClockSampler:
 
     def summary(self):
         sm, mx, reasons = [], None, set()
+        for f, m, rs in self.samples:
+            sm.append(f)
+            mx = m
+            reasons.update(rs)
         names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
         for line in (self.out or "").splitlines():
             f = [x.strip() for x in line.split(",")]
@@ -97,7 +134,8 @@ class ClockSampler:
                 if v.lower() == "active":
                     reasons.add(n)
         return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": mx,
-                "reasons": sorted(reasons), "samples": len(sm)}
+                "reasons": sorted(reasons), "samples": len(sm),
+                "source": "nvml" if self.nvml else "nvidia-smi"}
 
 
 def timed_steps(fn, steps, warmup, stream, flush=None):
@@ -347,9 +385,10 @@ def run_ours(args):
                     "d2h_bytes_per_step": nbytes},
             "roofline": {"bound": "hbm", "kernel": "dg_apply_kernel<3,1,false,double>",
                          "achieved": achieved_gbs, "peak": hbm, "unit": "GB/s",
-                         "frac": achieved_gbs / hbm, "traffic": None,
+                         "frac": achieved_gbs / hbm, "traffic": APPLY_TRAFFIC_BYTES,
                          "note": f"algorithmic bytes of one vmult ({alg_bytes:.4g} B) over the apply kernel's "
-                                 f"mean time; peak {peak_src}"},
+                                 f"mean time; peak {peak_src} (copy); traffic = dram bytes read + written per "
+                                 f"launch of the apply kernel in an ncu capture of this workload"},
             "fp64": {"achieved_tflops": flops / (vm_ms / 1e3) / 1e12, "peak_tflops_dgemm": fp64_peak,
                      "frac": (flops / (vm_ms / 1e3) / 1e12) / fp64_peak if fp64_peak else None,
                      "flops_per_vmult": flops},
