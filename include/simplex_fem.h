@@ -310,6 +310,23 @@ int fem_mg_set_learned_smoother(fem_mg* mg, fem_mlp* mlp, int32_t fallback);
 int fem_batch_create(fem_op* const* ops, int32_t n_ops, fem_batch** out);
 int fem_batch_destroy(fem_batch* batch);
 int fem_batch_vmult(fem_batch* batch, void* const* dst, const void* const* src, void* stream);
+int fem_batch_set_kernel_variant(fem_batch* batch, int32_t variant);
+
+/* ---- autotuner -------------------------------------------------------------
+ * Times every kernel variant (cells per CTA, thread or warp roles per cell;
+ * fem_op_params.kernel_variant) of an operator or a batch with CUDA events
+ * (median of `reps` launches after 2 warm-ups, on zero input), keeps the
+ * fastest and returns it in *variant.  us[3] receives the median time per
+ * variant (0 = not a candidate).  With use_cache != 0 a choice recorded for
+ * the same (kind, degree, precision, components, log2 cells, GPU name) is
+ * applied without timing (*cached = 1).  fem_autotune_cache sets a file that
+ * keeps the choices across processes (JSON lines; NULL = memory only).
+ * No counterpart in the reference (deal.II fixes its vectorisation at compile
+ * time).  Synchronises with the device; allocates two vectors per problem. */
+int fem_op_autotune(fem_op* op, int32_t reps, int32_t use_cache, int32_t* variant, int32_t* cached, double* us);
+int fem_batch_autotune(fem_batch* batch, int32_t reps, int32_t use_cache, int32_t* variant, int32_t* cached,
+                       double* us);
+int fem_autotune_cache(const char* path);
 
 #ifdef __cplusplus
 }

@@ -6,6 +6,7 @@
 
 #include "../../include/simplex_fem.h"
 #include "common.hpp"
+#include "autotune.hpp"
 #include "handles.hpp"
 
 namespace sfem {
@@ -265,6 +266,41 @@ int fem_batch_create(fem_op* const* ops, int32_t n_ops, fem_batch** out) {
 
 int fem_batch_destroy(fem_batch* batch) {
   return guarded([&] { delete batch; });
+}
+
+int fem_op_autotune(fem_op* op, int32_t reps, int32_t use_cache, int32_t* variant, int32_t* cached,
+                    double* us) {
+  return guarded([&] {
+    REQUIRE_PTR(op);
+    const sfem::TuneResult r = sfem::autotune(*op->op, reps, use_cache != 0);
+    if (variant) *variant = r.variant;
+    if (cached) *cached = r.cached ? 1 : 0;
+    if (us)
+      for (int i = 0; i < 3; ++i) us[i] = i < int(r.us.size()) ? r.us[i] : 0.0;
+  });
+}
+
+int fem_batch_autotune(fem_batch* batch, int32_t reps, int32_t use_cache, int32_t* variant, int32_t* cached,
+                       double* us) {
+  return guarded([&] {
+    REQUIRE_PTR(batch);
+    const sfem::TuneResult r = batch->batch->tune(reps, use_cache != 0);
+    if (variant) *variant = r.variant;
+    if (cached) *cached = r.cached ? 1 : 0;
+    if (us)
+      for (int i = 0; i < 3; ++i) us[i] = i < int(r.us.size()) ? r.us[i] : 0.0;
+  });
+}
+
+int fem_batch_set_kernel_variant(fem_batch* batch, int32_t variant) {
+  return guarded([&] {
+    REQUIRE_PTR(batch);
+    batch->batch->set_variant(variant);
+  });
+}
+
+int fem_autotune_cache(const char* path) {
+  return guarded([&] { sfem::tune_set_cache_file(path ? std::string(path) : std::string()); });
 }
 
 int fem_batch_vmult(fem_batch* batch, void* const* dst, const void* const* src, void* stream) {

@@ -6,6 +6,7 @@
 #include "kernels_cg.cuh"
 #include "kernels_dg.cuh"
 #include "kernels_dg3.cuh"
+#include "autotune.hpp"
 #include "operator.hpp"
 #include "ref_tables.h"
 
@@ -386,6 +387,62 @@ class DGBatchImpl final : public Batch {
     DGProblem<T> probs[kMaxBatch];
     for (size_t i = 0; i < ops.size(); ++i) probs[i] = ops[i]->problem(src[i], dst[i]);
     DGOperator<T>::launch_dg(cfg, probs, int(ops.size()), s, 0);
+  }
+  int variant() const override { return cfg.kernel_variant; }
+  void set_variant(int v) override {
+    SFEM_REQUIRE(v >= 0 && v <= 3, FEM_ERR_ARG, "batch: kernel variant must be 0..3");
+    cfg.kernel_variant = v;
+  }
+  TuneResult tune(int reps, bool use_cache) override {
+    TuneResult res;
+    res.us.assign(3, 0.0);
+    int64_t cells = 0;
+    for (auto* o : ops) cells += o->n_cells;
+    const std::string key = "batch" + std::to_string(ops.size()) + "," + tune_key(cfg, cells);
+    if (use_cache) {
+      const int v = tune_lookup(key);
+      if (v > 0) {
+        cfg.kernel_variant = v;
+        res.variant = v;
+        res.cached = true;
+        return res;
+      }
+    }
+    std::vector<DevBuf<T>> bufs;
+    std::vector<void*> d(ops.size());
+    std::vector<const void*> x(ops.size());
+    for (size_t i = 0; i < ops.size(); ++i) {
+      bufs.emplace_back(size_t(ops[i]->m));
+      bufs.emplace_back(size_t(ops[i]->m));
+      SFEM_CUDA(cudaMemset(bufs[2 * i].p, 0, sizeof(T) * ops[i]->m));
+    }
+    for (size_t i = 0; i < ops.size(); ++i) {
+      x[i] = bufs[2 * i].p;
+      d[i] = bufs[2 * i + 1].p;
+    }
+    cudaStream_t s = nullptr;
+    SFEM_CUDA(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking));
+    const int keep = cfg.kernel_variant;
+    double best = 1e300;
+    try {
+      for (int v : tune_candidates(cfg)) {
+        cfg.kernel_variant = v;
+        const double us = time_launches([&](cudaStream_t st) { vmult(d.data(), x.data(), st); }, reps, s);
+        res.us[v - 1] = us;
+        if (us < best) {
+          best = us;
+          res.variant = v;
+        }
+      }
+    } catch (...) {
+      cfg.kernel_variant = keep;
+      cudaStreamDestroy(s);
+      throw;
+    }
+    cudaStreamDestroy(s);
+    cfg.kernel_variant = res.variant;
+    tune_store(key, res.variant, res.us);
+    return res;
   }
 };
 

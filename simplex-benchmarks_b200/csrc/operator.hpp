@@ -110,11 +110,22 @@ double rhs_value(const RhsDesc& r, const double* x);
 
 std::unique_ptr<Operator> make_operator(const Mesh& mesh, const OpConfig& cfg);
 
+// Outcome of an autotuning run (autotune.hpp).
+struct TuneResult {
+  int variant = 0;
+  bool cached = false;
+  std::vector<double> us;  // median us per candidate (index = variant - 1), 0 = not timed
+};
+
 // Batched multi-problem DG launch.
 class Batch {
  public:
   virtual ~Batch() = default;
   virtual void vmult(void* const* dst, const void* const* src, cudaStream_t s) = 0;
+  // time the kernel variants on the whole batch and keep the fastest
+  virtual TuneResult tune(int reps, bool use_cache) = 0;
+  virtual int variant() const = 0;
+  virtual void set_variant(int v) = 0;
 };
 std::unique_ptr<Batch> make_batch(const std::vector<Operator*>& ops);
 

@@ -144,6 +144,12 @@ _PROTOS = [
     ("fem_batch_create", C.c_int, [C.c_void_p, C.c_int32, C.POINTER(C.c_void_p)]),
     ("fem_batch_destroy", C.c_int, [C.c_void_p]),
     ("fem_batch_vmult", C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]),
+    ("fem_batch_set_kernel_variant", C.c_int, [C.c_void_p, C.c_int32]),
+    ("fem_op_autotune", C.c_int, [C.c_void_p, C.c_int32, C.c_int32, C.POINTER(C.c_int32), C.POINTER(C.c_int32),
+                                  C.POINTER(C.c_double)]),
+    ("fem_batch_autotune", C.c_int, [C.c_void_p, C.c_int32, C.c_int32, C.POINTER(C.c_int32),
+                                     C.POINTER(C.c_int32), C.POINTER(C.c_double)]),
+    ("fem_autotune_cache", C.c_int, [C.c_char_p]),
 ]
 
 
@@ -310,6 +316,11 @@ class Operator:
     def set_kernel_variant(self, variant):
         check(lib().fem_op_set_kernel_variant(self.handle, variant))
 
+    def autotune(self, reps=20, use_cache=True):
+        """Time the kernel variants on this operator and keep the fastest
+        (fem_op_autotune); returns {"variant", "cached", "us": [per variant]}."""
+        return _autotune(lib().fem_op_autotune, self.handle, reps, use_cache)
+
     def work(self):
         f, b = C.c_double(), C.c_double()
         check(lib().fem_op_work(self.handle, C.byref(f), C.byref(b)))
@@ -340,10 +351,29 @@ class Batch:
         sa = (C.c_void_p * n)(*[s.data_ptr() for s in srcs])
         check(lib().fem_batch_vmult(self.handle, da, sa, _stream_ptr(stream)))
 
+    def set_kernel_variant(self, variant):
+        check(lib().fem_batch_set_kernel_variant(self.handle, variant))
+
+    def autotune(self, reps=20, use_cache=True):
+        """Time the kernel variants on the whole batch and keep the fastest."""
+        return _autotune(lib().fem_batch_autotune, self.handle, reps, use_cache)
+
     def __del__(self):
         if getattr(self, "handle", None) and _lib is not None:
             _lib.fem_batch_destroy(self.handle)
             self.handle = None
+
+
+def _autotune(fn, handle, reps, use_cache):
+    v, c = C.c_int32(), C.c_int32()
+    us = (C.c_double * 3)()
+    check(fn(handle, reps, int(bool(use_cache)), C.byref(v), C.byref(c), us))
+    return {"variant": v.value, "cached": bool(c.value), "us": list(us)}
+
+
+def set_autotune_cache(path):
+    """Keep autotuning choices in a JSON-lines file across processes (None: memory only)."""
+    check(lib().fem_autotune_cache(None if path is None else os.fsencode(path)))
 
 
 def rhs_desc(modes, kind=FEM_RHS_PLANE_WAVES):

@@ -152,3 +152,40 @@ def test_batch_matches_single(cuda, precision):
     o0 = orc.for_mesh(ops[2].mesh, 2, orc.HELMHOLTZ, n_components=3)
     x = srcs[2].double().cpu().numpy()
     assert rel_l2(outs[2].double().cpu().numpy(), o0.vmult(x)) <= TOL[precision]
+
+
+def test_autotuner_picks_a_variant_and_caches_it(cuda, tmp_path):
+    """The autotuner times the DG kernel variants, keeps the fastest, records it
+    in the cache file, and a second operator of the same shape reuses it; the
+    tuned operator still matches the oracle."""
+    sf.set_autotune_cache(str(tmp_path / "tune.jsonl"))
+    try:
+        mesh = sf.Mesh((6, 5, 4), jitter=0.1, seed=0)
+        op = sf.Operator(mesh, 3, "dg", "fp64")
+        r = op.autotune(reps=5)
+        assert r["variant"] in (1, 2, 3) and not r["cached"]
+        assert all(t > 0 for t in r["us"]) and r["us"][r["variant"] - 1] == min(r["us"])
+        op2 = sf.Operator(mesh, 3, "dg", "fp64")
+        r2 = op2.autotune(reps=5)
+        assert r2["cached"] and r2["variant"] == r["variant"]
+        assert (tmp_path / "tune.jsonl").read_text().count("variant") == 1
+        x = seeded_src(op.m(), 1)
+        ref = orc.for_mesh(mesh, 3, orc.DG).vmult(x)
+        assert rel_l2(run_product(op2, x), ref) <= 1e-12
+        # batch of uneven Helmholtz problems
+        import torch
+        meshes = [sf.Mesh(n) for n in (3, 4, 5)]
+        ops = [sf.Operator(m, 2, "helmholtz", "fp64") for m in meshes]
+        b = sf.Batch(ops)
+        rb = b.autotune(reps=3)
+        assert rb["variant"] in (1, 2, 3)
+        xs = [torch.tensor(seeded_src(o.m(), 7 + i), device="cuda") for i, o in enumerate(ops)]
+        ys = [o.initialize_dof_vector() for o in ops]
+        b.vmult(ys, xs)
+        for o, x_, y_ in zip(ops, xs, ys):
+            z = o.initialize_dof_vector()
+            o.vmult(z, x_)
+            torch.cuda.synchronize()
+            assert rel_l2(y_.cpu().numpy(), z.cpu().numpy()) <= 1e-13
+    finally:
+        sf.set_autotune_cache(None)
