@@ -47,6 +47,7 @@ def parse():
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-solve", action="store_true", help="skip the multigrid solve measurement")
+    ap.add_argument("--no-extra", action="store_true", help="skip the CG (configs 1, 1L) and batch (config 4) lines")
     return ap.parse_args()
 
 
@@ -231,6 +232,95 @@ def mg_solve_bench(repeats=5):
     return out
 
 
+def cg_vmult_bench(steps, warmup, flush):
+    """Config 1: CG P2 Poisson on 16^3 x 6 tets (jitter 0.1h, seed 0), src U[-1,1]
+    (seed 1) zeroed at constrained DoFs, FP64: 100 vmults replayed from one CUDA
+    graph, best of 5 replays.  Config 1L: CG P2 on 128^3 x 6 tets (16,974,593 DoFs),
+    FP64 and FP32, L2 flushed before every timed vmult: the HBM-bound case."""
+    import numpy as np
+    import torch
+    import simplexfem as sf
+    out = {}
+    s = torch.cuda.Stream()
+    mesh = sf.Mesh(16, jitter=JITTER, seed=0)
+    op = sf.Operator(mesh, 2, "cg", "fp64")
+    x = np.random.default_rng(1).uniform(-1.0, 1.0, op.m())
+    x[op.constrained().astype(bool)] = 0.0
+    src = torch.tensor(x, device="cuda")
+    dst = op.initialize_dof_vector()
+    with torch.cuda.stream(s):
+        for _ in range(3):
+            op.vmult(dst, src, s)
+    torch.cuda.synchronize()
+    g = torch.cuda.CUDAGraph()
+    with torch.cuda.graph(g, stream=s):
+        for _ in range(100):
+            op.vmult(dst, src, s)
+    best = 1e30
+    for _ in range(5):
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        with torch.cuda.stream(s):
+            a.record(s)
+            g.replay()
+            b.record(s)
+        torch.cuda.synchronize()
+        best = min(best, a.elapsed_time(b))
+    del g
+    out["config1"] = {"workload": "CG P2 Poisson vmult, 16^3 x 6 tets (24,576 cells, 35,937 DoFs), FP64, "
+                                  "100 vmults in one CUDA graph, best of 5",
+                      "dofs_per_s": 100 * op.m() / (best / 1e3), "us_per_vmult": best * 10.0}
+    del op, mesh
+    hbm, _ = measured_peaks()
+    mesh = sf.Mesh(128, jitter=JITTER, seed=0)
+    for prec in ("fp64", "fp32"):
+        op = sf.Operator(mesh, 2, "cg", prec)
+        src = torch.rand(op.m(), dtype=op.dtype, device="cuda") * 2 - 1
+        dst = op.initialize_dof_vector()
+        t = timed_steps(lambda: op.vmult(dst, src, s), steps, warmup, s, flush)
+        ms = statistics.mean(t)
+        _, alg = op.work()
+        out["config1L_" + prec] = {
+            "workload": "CG P2 Poisson vmult, 128^3 x 6 tets (12,582,912 cells, 16,974,593 DoFs), L2 flushed",
+            "dofs_per_s": op.m() / (ms / 1e3), "us_per_vmult": ms * 1e3,
+            "alg_gbs": alg / (ms / 1e3) / 1e9, "hbm_frac": alg / (ms / 1e3) / 1e9 / hbm}
+        del op, src, dst
+    return out
+
+
+def batch_bench(steps, warmup, flush):
+    """Config 4: 32 independent Helmholtz-like DG P2 x 3-component problems on
+    uneven meshes n_i = 8 + floor(32 i / 31) (8^3 .. 40^3 hexes x 6 tets,
+    110,213,460 DoFs in total), src_i ~ U[-1,1] (seeds 100 + i); one persistent
+    launch per pass for all 32, kernel shape picked by the autotuner; against the
+    same 32 vmults launched one after another."""
+    import numpy as np
+    import torch
+    import simplexfem as sf
+    sizes = [8 + (32 * i) // 31 for i in range(32)]
+    meshes = [sf.Mesh(n) for n in sizes]
+    s = torch.cuda.Stream()
+    out = {"workload": "32 Helmholtz DG P2 x 3 comps problems, n_i = 8 + floor(32 i/31) hexes/dir"}
+    for prec in ("fp64", "fp32"):
+        ops = [sf.Operator(m, 2, "helmholtz", prec) for m in meshes]
+        total = sum(o.m() for o in ops)
+        xs = [torch.tensor(np.random.default_rng(100 + i).uniform(-1.0, 1.0, o.m()), dtype=o.dtype, device="cuda")
+              for i, o in enumerate(ops)]
+        ys = [o.initialize_dof_vector() for o in ops]
+        b = sf.Batch(ops)
+        tune = b.autotune(reps=5, use_cache=False)
+        tb = timed_steps(lambda: b.vmult(ys, xs, s), steps, warmup, s, flush)
+
+        def one_by_one():
+            for o, x_, y_ in zip(ops, xs, ys):
+                o.vmult(y_, x_, s)
+        ts = timed_steps(one_by_one, steps, warmup, s, flush)
+        out[prec] = {"dofs": total, "batched_dofs_per_s": total / (statistics.mean(tb) / 1e3),
+                     "batched_ms": statistics.mean(tb), "sequential_ms": statistics.mean(ts),
+                     "autotuned_variant": tune["variant"], "variant_us": tune["us"]}
+        del ops, xs, ys, b
+    return out
+
+
 def cpu_baseline(mesh, x, target_seconds=12.0):
     """The oracle on this host's cores over a bounded slice of cells."""
     import numpy as np
@@ -372,6 +462,10 @@ def run_ours(args):
     vm_ms = statistics.mean(t64)
     fp64_peak = fp64_peak_tflops() if rank == 0 else None
     solve = mg_solve_bench() if (rank == 0 and not args.no_solve) else None
+    extra_cfg = None
+    if rank == 0 and not args.no_extra:
+        extra_cfg = cg_vmult_bench(min(args.steps, 100), 3, flush)
+        extra_cfg["config4"] = batch_bench(min(args.steps, 20), 3, flush)
 
     if rank == 0:
         line = {
@@ -396,6 +490,7 @@ def run_ours(args):
                            "vmult": vm_ms},
             "extra": {"fp32_value": value32, "fp32_ms_per_step": sum(t32) / args.steps},
             "solve": solve,
+            "configs": extra_cfg,
             "clocks": clk.summary(),
             "gpu_launches": 2 * args.steps,
         }
