@@ -145,7 +145,7 @@ __device__ __forceinline__ void issue_layer(const unsigned char* smem, uint32_t 
 // (J/h and 1/h), winv [m], r in, z += correction.  MODE 1: X [n][29] in
 // (passed as feat), O [n][20] out (passed as zout); dofs/winv/r unused.
 template <int MODE, typename T>
-__global__ void __launch_bounds__(128, 1) mlp_tc_kernel(int64_t n, const int32_t* __restrict__ dofs,
+__global__ void __launch_bounds__(128, 4) mlp_tc_kernel(int64_t n, const int32_t* __restrict__ dofs,
                                                         const float* __restrict__ feat,
                                                         const float* __restrict__ winv,
                                                         const __nv_bfloat16* __restrict__ wb,
@@ -204,7 +204,6 @@ __global__ void __launch_bounds__(128, 1) mlp_tc_kernel(int64_t n, const int32_t
     const bool live = c < n;
     // ---- input row
     float x[K1];
-    int32_t g[D::NR];
     float scale = 0.0f;
 #pragma unroll
     for (int i = 0; i < K1; ++i) x[i] = 0.0f;
@@ -212,8 +211,8 @@ __global__ void __launch_bounds__(128, 1) mlp_tc_kernel(int64_t n, const int32_t
       float s2 = 0.0f;
 #pragma unroll
       for (int i = 0; i < D::NR; ++i) {
-        g[i] = live ? __ldg(dofs + i * n + c) : -1;
-        x[i] = g[i] >= 0 ? float(r[g[i]]) : 0.0f;
+        const int32_t gi = live ? __ldg(dofs + i * n + c) : -1;
+        x[i] = gi >= 0 ? float(r[gi]) : 0.0f;
         s2 += x[i] * x[i];
       }
       if (s2 > 0.0f) {
@@ -235,7 +234,7 @@ __global__ void __launch_bounds__(128, 1) mlp_tc_kernel(int64_t n, const int32_t
     for (int ch = 0; ch < K1 / 8; ++ch) store_chunk(smem + OFF_X, t, ch, TILE, x + 8 * ch);
 
     // ---- three layers
-    float v[64];
+    float v[32];
 #pragma unroll 1
     for (int layer = 0; layer < 3; ++layer) {
       fence_async_smem();
@@ -254,28 +253,30 @@ __global__ void __launch_bounds__(128, 1) mlp_tc_kernel(int64_t n, const int32_t
         break;
       }
       tc_after_sync();
-      float a[32];
-      tmem_ld32(trow, a);
-#pragma unroll
-      for (int i = 0; i < 32; ++i) v[i] = a[i];
       if (layer < 2) {
-        tmem_ld32(trow + 32, a);
-#pragma unroll
-        for (int i = 0; i < 32; ++i) v[32 + i] = a[i];
+        // 32 accumulator columns at a time: bias, GELU, BF16 row chunks for the next layer
         const float* bias = sb + 64 * layer;
+#pragma unroll 1
+        for (int half = 0; half < 2; ++half) {
+          tmem_ld32(trow + 32 * half, v);
 #pragma unroll
-        for (int i = 0; i < 64; ++i) v[i] = gelu_fast(v[i] + bias[i]);
+          for (int i = 0; i < 32; ++i) v[i] = gelu_fast(v[i] + bias[32 * half + i]);
 #pragma unroll
-        for (int ch = 0; ch < 8; ++ch) store_chunk(smem + OFF_H, t, ch, TILE, v + 8 * ch);
+          for (int ch = 0; ch < 4; ++ch) store_chunk(smem + OFF_H, t, 4 * half + ch, TILE, v + 8 * ch);
+        }
+      } else {
+        tmem_ld32(trow, v);
       }
     }
     if (failed) break;
-    // ---- output row
+    // ---- output row (the DoF indices are read again: they are still in L2)
     if (MODE == 0) {
       if (scale != 0.0f) {
 #pragma unroll
-        for (int i = 0; i < D::NR; ++i)
-          if (g[i] >= 0) atomicAdd(z + g[i], T(scale * (v[i] + sb[128 + i]) * __ldg(winv + g[i])));
+        for (int i = 0; i < D::NR; ++i) {
+          const int32_t gi = __ldg(dofs + i * n + c);
+          if (gi >= 0) atomicAdd(z + gi, T(scale * (v[i] + sb[128 + i]) * __ldg(winv + gi)));
+        }
       }
     } else if (live) {
 #pragma unroll
