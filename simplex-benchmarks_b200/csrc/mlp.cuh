@@ -32,11 +32,13 @@ __device__ __forceinline__ float gelu_grad(float x) {
   return 0.5f * (1.0f + t) + 0.5f * x * (1.0f - t * t) * 0.7978845608028654f * (1.0f + 0.134145f * x * x);
 }
 // the same GELU with the hardware tanh approximation (tensor-core epilogues)
+// (6 instructions: u = x (c1 + c2 x^2), y = h + h tanh(u), h = x / 2)
 __device__ __forceinline__ float gelu_fast(float x) {
-  const float u = 0.7978845608028654f * (x + 0.044715f * x * x * x);
+  const float u = x * fmaf(0.7978845608028654f * 0.044715f, x * x, 0.7978845608028654f);
   float t;
   asm("tanh.approx.f32 %0, %1;" : "=f"(t) : "f"(u));
-  return 0.5f * x * (1.0f + t);
+  const float h = 0.5f * x;
+  return fmaf(h, t, h);
 }
 
 // FP32 master -> BF16 image

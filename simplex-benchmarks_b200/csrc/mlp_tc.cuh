@@ -246,7 +246,12 @@ __global__ void __launch_bounds__(128, 4) mlp_tc_kernel(int64_t n, const int32_t
         else if (layer == 1) issue_layer(smem, tmem, OFF_H, OFF_W2, 64, 64, bar);
         else issue_layer(smem, tmem, OFF_H, OFF_W3, 64, N3, bar);
       }
-      const bool ok = bar_wait(bar, phase);
+      // one thread polls the mbarrier; the others wait at the block barrier
+      bool ok = true;
+      if (t == 0) {
+        ok = bar_wait(bar, phase);
+        tc_before_sync();
+      }
       phase ^= 1u;
       if (__syncthreads_or(!ok)) {
         failed = true;
@@ -259,8 +264,15 @@ __global__ void __launch_bounds__(128, 4) mlp_tc_kernel(int64_t n, const int32_t
 #pragma unroll 1
         for (int half = 0; half < 2; ++half) {
           tmem_ld32(trow + 32 * half, v);
+          const float4* b4 = reinterpret_cast<const float4*>(bias + 32 * half);
 #pragma unroll
-          for (int i = 0; i < 32; ++i) v[i] = gelu_fast(v[i] + bias[32 * half + i]);
+          for (int q = 0; q < 8; ++q) {
+            const float4 bq = b4[q];
+            v[4 * q] = gelu_fast(v[4 * q] + bq.x);
+            v[4 * q + 1] = gelu_fast(v[4 * q + 1] + bq.y);
+            v[4 * q + 2] = gelu_fast(v[4 * q + 2] + bq.z);
+            v[4 * q + 3] = gelu_fast(v[4 * q + 3] + bq.w);
+          }
 #pragma unroll
           for (int ch = 0; ch < 4; ++ch) store_chunk(smem + OFF_H, t, 4 * half + ch, TILE, v + 8 * ch);
         }
@@ -270,17 +282,28 @@ __global__ void __launch_bounds__(128, 4) mlp_tc_kernel(int64_t n, const int32_t
     }
     if (failed) break;
     // ---- output row (the DoF indices are read again: they are still in L2)
+    {
+      const float4* b4 = reinterpret_cast<const float4*>(sb + 128);
+#pragma unroll
+      for (int q = 0; q < D::NOUT / 4; ++q) {
+        const float4 bq = b4[q];
+        v[4 * q] += bq.x;
+        v[4 * q + 1] += bq.y;
+        v[4 * q + 2] += bq.z;
+        v[4 * q + 3] += bq.w;
+      }
+    }
     if (MODE == 0) {
       if (scale != 0.0f) {
 #pragma unroll
         for (int i = 0; i < D::NR; ++i) {
           const int32_t gi = __ldg(dofs + i * n + c);
-          if (gi >= 0) atomicAdd(z + gi, T(scale * (v[i] + sb[128 + i]) * __ldg(winv + gi)));
+          if (gi >= 0) atomicAdd(z + gi, T(scale * v[i] * __ldg(winv + gi)));
         }
       }
     } else if (live) {
 #pragma unroll
-      for (int j = 0; j < D::NOUT; ++j) zout[c * D::NOUT + j] = v[j] + sb[128 + j];
+      for (int j = 0; j < D::NOUT; ++j) zout[c * D::NOUT + j] = v[j];
     }
     // the next tile's layer-1 MMA overwrites the accumulator read above
     tc_before_sync();
