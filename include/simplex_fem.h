@@ -199,7 +199,8 @@ typedef struct fem_mg_params {
   int32_t c_transfer;       /* FEM_DG fine operators: 0 = DG P_p .. P_1 then CG P_1 (phc),
                                1 = CG P_p right below DG P_p, then the CG ladder of `order`
                                (cph / chp; DG/cells_batched/application_phc.cc:3396-3652) */
-  int32_t reserved[3];
+  int32_t learned_steps;    /* learned finest-level smoothing per V-cycle: 1 pre, 2 post, 3 both (3) */
+  int32_t reserved[2];
 } fem_mg_params;
 int fem_mg_params_default(fem_mg_params* p);
 int fem_mg_create(fem_op* fine, const fem_mg_params* p, fem_mg** out);

@@ -747,10 +747,14 @@ class MultigridImpl final : public Multigrid {
     const unsigned g = grid_for(m);
     const bool learned = use_learned_ && l == int(levels_.size()) - 1;
     if (learned) {
-      // pre-smoothing from zero: x = w z, z = S(b), w = (b,z)/(z,Az); r = b - w Az
       SFEM_CUDA(cudaMemsetAsync(L.x.p, 0, sizeof(T) * m, s));
-      learned_step(L, L.b.p, s);
-      residual_ratio<T><<<g, 256, 0, s>>>(m, step_.p, L.b.p, L.t.p, L.r.p);
+      if (params.learned_steps & 1) {
+        // pre-smoothing from zero: x = w z, z = S(b), w = (b,z)/(z,Az); r = b - w Az
+        learned_step(L, L.b.p, s);
+        residual_ratio<T><<<g, 256, 0, s>>>(m, step_.p, L.b.p, L.t.p, L.r.p);
+      } else {
+        SFEM_CUDA(cudaMemcpyAsync(L.r.p, L.b.p, sizeof(T) * m, cudaMemcpyDeviceToDevice, s));
+      }
     } else {
       smooth(l, L.x.p, L.b.p, true, s);
       L.op->vmult(L.t.p, L.x.p, s);
@@ -762,6 +766,7 @@ class MultigridImpl final : public Multigrid {
     cycle(l - 1, s);
     prolongate_add(l, L.x.p, C.x.p, s);
     if (learned) {
+      if (!(params.learned_steps & 2)) return;
       // post-smoothing: one energy-optimal step along S(b - A x)
       L.op->vmult(L.t.p, L.x.p, s);
       vec_residual<T><<<g, 256, 0, s>>>(m, L.b.p, L.t.p, L.r.p);

@@ -30,6 +30,8 @@ struct MGParams {
   // reference's phc order); 1: CG P_p right below DG P_p, then the CG p/h
   // ladder of `order` (cph with FEM_MG_PH, chp with FEM_MG_HP).
   int c_transfer = 0;
+  // finest-level learned smoothing steps per V-cycle: 1 pre, 2 post, 3 both
+  int learned_steps = 3;
 };
 
 class Multigrid {

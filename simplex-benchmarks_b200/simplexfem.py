@@ -49,7 +49,7 @@ class MGParams(C.Structure):
     _fields_ = [("order", C.c_int32), ("precision", C.c_int32), ("smoother_degree", C.c_int32),
                 ("eig_iterations", C.c_int32), ("smoothing_range", C.c_double), ("eig_safety", C.c_double),
                 ("coarse_n", C.c_int32), ("use_graph", C.c_int32), ("c_transfer", C.c_int32),
-                ("reserved", C.c_int32 * 3)]
+                ("learned_steps", C.c_int32), ("reserved", C.c_int32 * 2)]
 
 
 class SolveInfo(C.Structure):
@@ -412,7 +412,7 @@ class Multigrid:
     c_transfer=1 hands over at P_p (cph with FEM_MG_PH, chp with FEM_MG_HP)."""
 
     def __init__(self, fine_op, order=FEM_MG_PH, precision="fp32", smoother_degree=3, smoothing_range=20.0,
-                 eig_iterations=10, eig_safety=1.2, coarse_n=4, use_graph=True, c_transfer=0):
+                 eig_iterations=10, eig_safety=1.2, coarse_n=4, use_graph=True, c_transfer=0, learned_steps=3):
         p = MGParams()
         check(lib().fem_mg_params_default(C.byref(p)))
         p.order = order
@@ -424,6 +424,7 @@ class Multigrid:
         p.coarse_n = coarse_n
         p.use_graph = int(bool(use_graph))
         p.c_transfer = c_transfer
+        p.learned_steps = learned_steps
         h = C.c_void_p()
         check(lib().fem_mg_create(fine_op.handle, C.byref(p), C.byref(h)))
         self.handle = h
