@@ -81,7 +81,10 @@ typedef struct fem_op_params {
   int32_t n_components;    /* FEM_HELMHOLTZ: number of fields (reference: 3); others: 1 */
   int32_t penalty;         /* FEM_DG: enum fem_penalty */
   int32_t kernel_variant;  /* 0: tuned default; DG/Helmholtz: 1 thread per cell x128 cells per
-                              CTA, 2 thread per cell x64, 3 warp roles x32 (autotuner knob) */
+                              CTA, 2 thread per cell x64, 3 warp roles x32; CG: 1 thread per
+                              cell (default for P3), 2 thread per Kuhn hex (6 tets, one atomic
+                              per distinct DoF; default for P1/P2; the cell kernel where the
+                              mesh has no hex pattern) */
   int32_t reserved[5];
 } fem_op_params;
 

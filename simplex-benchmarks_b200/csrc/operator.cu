@@ -59,6 +59,72 @@ class CGOperator final : public Operator {
   DevBuf<int32_t> d_dofs;        // [K][n_cells], -1 = constrained
   DevBuf<T> d_geo;               // [6][n_cells]
   DevBuf<int32_t> d_constrained; // constrained DoF list
+  // macro-element (hex) tables of cg_hex_kernel; empty when the mesh is not
+  // 6 consecutive Kuhn tets per hex with one common DoF pattern
+  DevBuf<int32_t> d_hdofs;       // [H][n_hex]
+  DevBuf<T> d_hgeo;              // [36][n_hex]: metric of tet q at rows 6 q .. 6 q + 5
+  HexMap hex_map{};
+  int64_t n_hex = 0;
+  int hex_H = 0;
+
+  static int hex_dofs(int p) { return p == 1 ? 8 : p == 2 ? 27 : 64; }
+
+  void build_hex_tables(const Mesh& mesh, const CGDofs& dofs, const std::vector<T>& geo) {
+    if (n_cells == 0 || n_cells % 6 != 0 || int64_t(mesh.cell_hex.size()) != n_cells) return;
+    const int64_t nh = n_cells / 6;
+    const int H = hex_dofs(cfg.degree);
+    // hex-local numbering by first occurrence over (tet, local DoF)
+    auto local_map = [&](int64_t h, int8_t (&mm)[6][20], std::vector<int32_t>& order) -> bool {
+      order.clear();
+      for (int q = 0; q < 6; ++q) {
+        if (mesh.cell_hex[6 * h + q] != mesh.cell_hex[6 * h]) return false;
+        for (int i = 0; i < K; ++i) {
+          const int32_t g = dofs.cell_dofs[size_t(K) * (6 * h + q) + i];
+          int k = 0;
+          while (k < int(order.size()) && order[k] != g) ++k;
+          if (k == int(order.size())) {
+            if (k >= H) return false;
+            order.push_back(g);
+          }
+          mm[q][i] = int8_t(k);
+        }
+      }
+      return int(order.size()) == H;
+    };
+    HexMap m0{};
+    std::vector<int32_t> ord0;
+    if (!local_map(0, m0.m, ord0)) return;
+    std::vector<int32_t> hd(size_t(H) * nh);
+    bool ok = true;
+#pragma omp parallel
+    {
+      std::vector<int32_t> ord;
+      int8_t mm[6][20];
+#pragma omp for schedule(static)
+      for (int64_t h = 0; h < nh; ++h) {
+        if (!ok) continue;
+        bool same = local_map(h, mm, ord);
+        for (int q = 0; q < 6 && same; ++q)
+          for (int i = 0; i < K; ++i) same = same && mm[q][i] == m0.m[q][i];
+        if (!same) {
+          ok = false;
+          continue;
+        }
+        for (int k = 0; k < H; ++k) hd[size_t(k) * nh + h] = dofs.constrained[ord[k]] ? -1 : ord[k];
+      }
+    }
+    if (!ok) return;
+    std::vector<T> hg(36 * size_t(nh));
+#pragma omp parallel for schedule(static)
+    for (int64_t h = 0; h < nh; ++h)
+      for (int q = 0; q < 6; ++q)
+        for (int k = 0; k < 6; ++k) hg[size_t(6 * q + k) * nh + h] = geo[size_t(k) * n_cells + 6 * h + q];
+    d_hgeo.upload(hg);
+    d_hdofs.upload(hd);
+    hex_map = m0;
+    n_hex = nh;
+    hex_H = H;
+  }
 
   CGOperator(const Mesh& mesh, const OpConfig& c) {
     cfg = c;
@@ -89,6 +155,29 @@ class CGOperator final : public Operator {
     for (int64_t i = 0; i < m; ++i)
       if (constrained[i]) cl.push_back(int32_t(i));
     d_constrained.upload(cl);
+    build_hex_tables(mesh, dofs, geo);
+    if (hex_H) {
+      switch (cfg.degree) {
+        case 1: setup_hex<1, 8>(); break;
+        case 2: setup_hex<2, 27>(); break;
+        case 3: setup_hex<3, 64>(); break;
+      }
+    }
+  }
+
+  static constexpr int kHexBS = 64;
+  template <int P, int H>
+  static size_t hex_smem() { return 2 * size_t(kHexBS) * HexRow<H>::S * sizeof(T); }
+  template <int P, int H>
+  void setup_hex() {
+    SFEM_CUDA(cudaFuncSetAttribute(cg_hex_kernel<P, T, H, kHexBS>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                   int(hex_smem<P, H>())));
+  }
+  template <int P, int H>
+  void launch_hex(const T* x, T* d, cudaStream_t s) {
+    const unsigned grid = blocks_for(std::max<int64_t>(n_hex, 1), kHexBS);
+    cg_hex_kernel<P, T, H, kHexBS><<<grid, kHexBS, hex_smem<P, H>(), s>>>(
+        n_hex, d_hdofs.p, hex_map, d_hgeo.p, x, d, d_constrained.n, d_constrained.p);
   }
 
   void vmult(void* dst, const void* src, cudaStream_t s) override {
@@ -101,6 +190,19 @@ class CGOperator final : public Operator {
     const T* x = static_cast<const T*>(src);
     if (phase == 1) {
       SFEM_CUDA(cudaMemsetAsync(d, 0, sizeof(T) * m, s));
+      return;
+    }
+    // variant 2 (and the default for P1/P2; measured on B200, P3 runs better
+    // per cell): one thread per hex, or the cell kernel on meshes without the
+    // common hex pattern
+    const bool hex = hex_H && (cfg.kernel_variant == 2 || (cfg.kernel_variant == 0 && cfg.degree <= 2));
+    if (hex) {
+      switch (cfg.degree) {
+        case 1: launch_hex<1, 8>(x, d, s); break;
+        case 2: launch_hex<2, 27>(x, d, s); break;
+        case 3: launch_hex<3, 64>(x, d, s); break;
+      }
+      SFEM_CUDA(cudaGetLastError());
       return;
     }
     const int64_t n = std::max<int64_t>(n_cells, int64_t(d_constrained.n));

@@ -46,6 +46,21 @@ def test_vmult_parity_small(cuda, p, kind, precision):
     assert rel_l2(y, ref) <= TOL[precision]
 
 
+@pytest.mark.parametrize("precision", ["fp64", "fp32"])
+@pytest.mark.parametrize("variant", [1, 2])
+@pytest.mark.parametrize("p", [1, 2, 3])
+def test_cg_kernel_variants(cuda, p, variant, precision):
+    """Thread-per-cell (1) and thread-per-hex (2, one atomic per distinct DoF of
+    the hex's 6 tets) CG kernels against the oracle."""
+    mesh = sf.Mesh((6, 5, 7), jitter=0.1, seed=3)
+    op = sf.Operator(mesh, p, "cg", precision)
+    op.set_kernel_variant(variant)
+    x = seeded_src(op.m(), 1)
+    y = run_product(op, x)
+    ref = orc.for_mesh(mesh, p, orc.CG).vmult(oracle_input(op, x))
+    assert rel_l2(y, ref) <= TOL[precision]
+
+
 def test_config1_cg_p2_full_size(cuda):
     """16^3 x 6 tets, CG P2, jitter 0.1 (seed 0), src U[-1,1] (seed 1), FP64."""
     mesh = sf.Mesh(16, jitter=0.1, seed=0)
