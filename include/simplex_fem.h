@@ -82,9 +82,10 @@ typedef struct fem_op_params {
   int32_t penalty;         /* FEM_DG: enum fem_penalty */
   int32_t kernel_variant;  /* 0: tuned default; DG/Helmholtz: 1 thread per cell x128 cells per
                               CTA, 2 thread per cell x64, 3 warp roles x32; CG: 1 thread per
-                              cell (default for P3), 2 thread per Kuhn hex (6 tets, one atomic
-                              per distinct DoF; default for P1/P2; the cell kernel where the
-                              mesh has no hex pattern) */
+                              cell, 2 thread per Kuhn hex (6 tets, one atomic per distinct
+                              DoF), 3 CTA per 4x4x4-hex Morton cube (stores for cube-interior
+                              DoFs); each falls back to the next simpler form where the mesh
+                              lacks the pattern; default P1 2, P2 3, P3 3 (FP32) / 1 (FP64) */
   int32_t reserved[5];
 } fem_op_params;
 

@@ -46,7 +46,7 @@ void load_file_locked() {
 }  // namespace
 
 std::vector<int> tune_candidates(const OpConfig& cfg) {
-  if (cfg.kind == FEM_CG) return {1, 2};
+  if (cfg.kind == FEM_CG) return {1, 2, 3};
   return {1, 2, 3};
 }
 

@@ -146,6 +146,77 @@ __global__ void __launch_bounds__(BS) cg_hex_kernel(int64_t n_hex, const int32_t
   }
 }
 
+// Cube-block form for Kuhn meshes whose hexes come in Morton order: 64
+// consecutive hexes (384 tets) form a 4 x 4 x 4 cube, and every cube has the
+// same local structure, so one set of small tables serves all blocks.  One
+// CTA per cube, one thread per tet:
+//   1. the cube's distinct DoFs (P1 125, P2 729) are gathered once into
+//      shared memory;
+//   2. each thread applies its tet's operator and writes the 20-or-fewer
+//      results to its shared-memory row;
+//   3. each distinct DoF sums its contributions (work split among the threads
+//      longest-first, so every thread sums ~K values) and is written back
+//      once: a plain store when only this cube touches it, else one atomic.
+// About 6 atomics per hex for P2 (27 with cg_hex_kernel, 60 with
+// cg_cell_kernel) and one gather per distinct DoF.
+// tmap  [384][K] cube-local DoF of tet t's local DoF i
+// bdof  [n_blocks][NB] global DoF | (interior << 30), -1 at constrained DoFs
+// rptr  [385], rdof: the cube DoFs thread t reduces (rdof[rptr[t] .. rptr[t+1]))
+// cptr  [NB+1], cslot: row slots (t * KP + i) holding the contributions of DoF j
+template <int P, typename T, int NB, int KP>
+__global__ void __launch_bounds__(384) cg_cube_kernel(int64_t n_blocks, const int16_t* __restrict__ tmap,
+                                                      const int32_t* __restrict__ bdof,
+                                                      const int16_t* __restrict__ rptr,
+                                                      const int16_t* __restrict__ rdof,
+                                                      const int16_t* __restrict__ cptr,
+                                                      const int16_t* __restrict__ cslot,
+                                                      const T* __restrict__ geo, const T* __restrict__ src,
+                                                      T* __restrict__ dst, int64_t n_constrained,
+                                                      const int32_t* __restrict__ constrained) {
+  using O = gen::Ops<P>;
+  constexpr int K = O::K;
+  extern __shared__ __align__(16) unsigned char smem_cube[];
+  T* ub = reinterpret_cast<T*>(smem_cube);  // [NB]
+  T* yr = ub + NB;                          // [384][KP]
+  const int t = threadIdx.x;
+  const int64_t b = blockIdx.x;
+  for (int64_t i = b * 384 + t; i < n_constrained; i += int64_t(gridDim.x) * 384) {
+    const int32_t g = constrained[i];
+    dst[g] = src[g];
+  }
+  const int32_t* bd = bdof + b * NB;
+  for (int j = t; j < NB; j += 384) {
+    const int32_t code = __ldg(bd + j);
+    ub[j] = code >= 0 ? __ldg(src + (code & 0x3FFFFFFF)) : T(0);
+  }
+  __syncthreads();
+  {
+    const int64_t n_cells = n_blocks * 384;
+    const int64_t c = b * 384 + t;
+    T G[6], ut[K], yt[K];
+#pragma unroll
+    for (int k = 0; k < 6; ++k) G[k] = __ldg(geo + k * n_cells + c);
+#pragma unroll
+    for (int i = 0; i < K; ++i) ut[i] = ub[__ldg(tmap + t * K + i)];
+    cg_local_apply<P>(G, ut, yt);
+#pragma unroll
+    for (int i = 0; i < K; ++i) yr[t * KP + i] = yt[i];
+  }
+  __syncthreads();
+  const int r1 = __ldg(rptr + t + 1);
+  for (int r = __ldg(rptr + t); r < r1; ++r) {
+    const int j = __ldg(rdof + r);
+    const int32_t code = __ldg(bd + j);
+    if (code < 0) continue;
+    T s = T(0);
+    const int e1 = __ldg(cptr + j + 1);
+    for (int e = __ldg(cptr + j); e < e1; ++e) s += yr[__ldg(cslot + e)];
+    const int32_t g = code & 0x3FFFFFFF;
+    if (code & 0x40000000) dst[g] = s;
+    else atomicAdd(dst + g, s);
+  }
+}
+
 // Diagonal of the assembled operator: sum over cells of (A_K)_ii, constrained
 // rows get 1 (ones on the diagonal).  dst zero on entry.
 template <int P, typename T>

@@ -2,6 +2,7 @@
 #include <algorithm>
 #include <cmath>
 #include <cstring>
+#include <unordered_map>
 
 #include "kernels_cg.cuh"
 #include "kernels_dg.cuh"
@@ -68,6 +69,119 @@ class CGOperator final : public Operator {
   int hex_H = 0;
 
   static int hex_dofs(int p) { return p == 1 ? 8 : p == 2 ? 27 : 64; }
+
+  // cube-block tables of cg_cube_kernel (blocks of 64 hexes = 384 tets)
+  DevBuf<int16_t> d_tmap, d_rptr, d_rdof, d_cptr, d_cslot;
+  DevBuf<int32_t> d_bdof;
+  int64_t n_blocks = 0;
+  int cube_NB = 0;
+  static int cube_nb(int p) { return p == 1 ? 125 : p == 2 ? 729 : 2197; }
+  static int cube_kp(int k) { return (k % 2) ? k : k + 1; }
+
+  void build_cube_tables(const CGDofs& dofs) {
+    if (n_cells == 0 || n_cells % 384 != 0) return;
+    const int NB = cube_nb(cfg.degree), KP = cube_kp(K);
+    const int64_t nbk = n_cells / 384;
+    // cube-local numbering by first occurrence over (tet, local DoF)
+    auto local = [&](int64_t b, std::vector<int16_t>& tm, std::vector<int32_t>& order,
+                     std::unordered_map<int32_t, int>& at) -> bool {
+      order.clear();
+      at.clear();
+      tm.resize(size_t(384) * K);
+      for (int t = 0; t < 384; ++t)
+        for (int i = 0; i < K; ++i) {
+          const int32_t g = dofs.cell_dofs[size_t(K) * (384 * b + t) + i];
+          auto it = at.find(g);
+          int j;
+          if (it == at.end()) {
+            j = int(order.size());
+            if (j >= NB) return false;
+            at.emplace(g, j);
+            order.push_back(g);
+          } else {
+            j = it->second;
+          }
+          tm[t * K + i] = int16_t(j);
+        }
+      return int(order.size()) == NB;
+    };
+    std::vector<int16_t> tm0;
+    std::vector<int32_t> ord0;
+    std::unordered_map<int32_t, int> at0;
+    if (!local(0, tm0, ord0, at0)) return;
+    // contribution lists and their sizes (identical in every block)
+    std::vector<std::vector<int16_t>> contrib(NB);
+    for (int t = 0; t < 384; ++t)
+      for (int i = 0; i < K; ++i) contrib[tm0[t * K + i]].push_back(int16_t(t * KP + i));
+    std::vector<int32_t> count(m, 0);
+    for (size_t i = 0; i < dofs.cell_dofs.size(); ++i) ++count[dofs.cell_dofs[i]];
+    std::vector<int32_t> bd(size_t(NB) * nbk);
+    bool ok = true;
+#pragma omp parallel
+    {
+      std::vector<int16_t> tm;
+      std::vector<int32_t> ord;
+      std::unordered_map<int32_t, int> at;
+      at.reserve(4 * NB);
+#pragma omp for schedule(dynamic, 16)
+      for (int64_t b = 0; b < nbk; ++b) {
+        if (!ok) continue;
+        if (!local(b, tm, ord, at) || tm != tm0) {
+          ok = false;
+          continue;
+        }
+        for (int j = 0; j < NB; ++j) {
+          const int32_t g = ord[j];
+          const bool interior = count[g] == int(contrib[j].size());
+          bd[size_t(b) * NB + j] = dofs.constrained[g] ? -1 : (g | (interior ? 0x40000000 : 0));
+        }
+      }
+    }
+    if (!ok || m >= (int64_t(1) << 30)) return;
+    // reduce work: DoFs dealt longest-first to the least-loaded thread
+    std::vector<int> jorder(NB);
+    for (int j = 0; j < NB; ++j) jorder[j] = j;
+    std::stable_sort(jorder.begin(), jorder.end(),
+                     [&](int a, int b2) { return contrib[a].size() > contrib[b2].size(); });
+    std::vector<std::vector<int16_t>> per(384);
+    std::vector<int> load(384, 0);
+    for (int j : jorder) {
+      const int th = int(std::min_element(load.begin(), load.end()) - load.begin());
+      per[th].push_back(int16_t(j));
+      load[th] += int(contrib[j].size()) + 2;
+    }
+    std::vector<int16_t> rptr(385, 0), rdof, cptr(NB + 1, 0), cslot;
+    for (int th = 0; th < 384; ++th) {
+      rptr[th + 1] = int16_t(rptr[th] + per[th].size());
+      rdof.insert(rdof.end(), per[th].begin(), per[th].end());
+    }
+    for (int j = 0; j < NB; ++j) {
+      cptr[j + 1] = int16_t(cptr[j] + contrib[j].size());
+      cslot.insert(cslot.end(), contrib[j].begin(), contrib[j].end());
+    }
+    d_tmap.upload(tm0);
+    d_rptr.upload(rptr);
+    d_rdof.upload(rdof);
+    d_cptr.upload(cptr);
+    d_cslot.upload(cslot);
+    d_bdof.upload(bd);
+    n_blocks = nbk;
+    cube_NB = NB;
+  }
+
+  template <int P, int NB, int KP>
+  static size_t cube_smem() { return (size_t(NB) + 384 * size_t(KP)) * sizeof(T); }
+  template <int P, int NB, int KP>
+  void setup_cube() {
+    SFEM_CUDA(cudaFuncSetAttribute(cg_cube_kernel<P, T, NB, KP>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                   int(cube_smem<P, NB, KP>())));
+  }
+  template <int P, int NB, int KP>
+  void launch_cube(const T* x, T* d, cudaStream_t s) {
+    cg_cube_kernel<P, T, NB, KP><<<unsigned(n_blocks), 384, cube_smem<P, NB, KP>(), s>>>(
+        n_blocks, d_tmap.p, d_bdof.p, d_rptr.p, d_rdof.p, d_cptr.p, d_cslot.p, d_geo.p, x, d, d_constrained.n,
+        d_constrained.p);
+  }
 
   void build_hex_tables(const Mesh& mesh, const CGDofs& dofs, const std::vector<T>& geo) {
     if (n_cells == 0 || n_cells % 6 != 0 || int64_t(mesh.cell_hex.size()) != n_cells) return;
@@ -156,6 +270,14 @@ class CGOperator final : public Operator {
       if (constrained[i]) cl.push_back(int32_t(i));
     d_constrained.upload(cl);
     build_hex_tables(mesh, dofs, geo);
+    build_cube_tables(dofs);
+    if (cube_NB) {
+      switch (cfg.degree) {
+        case 1: setup_cube<1, 125, 5>(); break;
+        case 2: setup_cube<2, 729, 11>(); break;
+        case 3: setup_cube<3, 2197, 21>(); break;
+      }
+    }
     if (hex_H) {
       switch (cfg.degree) {
         case 1: setup_hex<1, 8>(); break;
@@ -192,11 +314,22 @@ class CGOperator final : public Operator {
       SFEM_CUDA(cudaMemsetAsync(d, 0, sizeof(T) * m, s));
       return;
     }
-    // variant 2 (and the default for P1/P2; measured on B200, P3 runs better
-    // per cell): one thread per hex, or the cell kernel on meshes without the
-    // common hex pattern
-    const bool hex = hex_H && (cfg.kernel_variant == 2 || (cfg.kernel_variant == 0 && cfg.degree <= 2));
-    if (hex) {
+    // default (variant 0), measured on B200: P1 per hex, P2 per cube, P3 per
+    // cube in FP32 and per cell in FP64
+    int v = cfg.kernel_variant;
+    if (v == 0) v = cfg.degree == 1 ? 2 : cfg.degree == 2 ? 3 : (sizeof(T) == 4 ? 3 : 1);
+    if (v == 3 && cube_NB) {
+      switch (cfg.degree) {
+        case 1: launch_cube<1, 125, 5>(x, d, s); break;
+        case 2: launch_cube<2, 729, 11>(x, d, s); break;
+        case 3: launch_cube<3, 2197, 21>(x, d, s); break;
+      }
+      SFEM_CUDA(cudaGetLastError());
+      return;
+    }
+    // variant 2 (and 3 without whole cubes): one thread per hex; the cell
+    // kernel on meshes without the common hex pattern
+    if ((v == 2 || v == 3) && hex_H) {
       switch (cfg.degree) {
         case 1: launch_hex<1, 8>(x, d, s); break;
         case 2: launch_hex<2, 27>(x, d, s); break;
