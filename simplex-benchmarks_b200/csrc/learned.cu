@@ -27,8 +27,8 @@ __global__ void gather_rows(int n, int width, const int32_t* __restrict__ perm, 
   out[t] = in[int64_t(perm[r]) * width + c];
 }
 
-// persistent tensor-core launch: 5 CTAs per SM (each holds 64 of the 512
-// tensor-memory columns and 41.6 KB of shared memory; 79 registers)
+// persistent tensor-core launch: 2 CTAs of 4 groups per SM (each CTA holds
+// 256 of the 512 tensor-memory columns and 89 KB of shared memory)
 template <int MODE, typename T>
 void launch_tc(int64_t n, const int32_t* dofs, const float* feat, const float* winv, const __nv_bfloat16* wb,
                const T* r, T* z, float* zout, int* status, cudaStream_t s) {
@@ -42,8 +42,9 @@ void launch_tc(int64_t n, const int32_t* dofs, const float* feat, const float* w
   SFEM_CUDA(cudaGetDevice(&dev));
   SFEM_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
   const int64_t tiles = (n + tc::TILE - 1) / tc::TILE;
-  const unsigned grid = unsigned(std::max<int64_t>(1, std::min<int64_t>(tiles, int64_t(sms) * 5)));
-  kern<<<grid, 128, tc::SMEM_BYTES, s>>>(n, dofs, feat, winv, wb, r, z, zout, status);
+  const int64_t groups = (tiles + tc::GROUPS - 1) / tc::GROUPS;
+  const unsigned grid = unsigned(std::max<int64_t>(1, std::min<int64_t>(groups, int64_t(sms) * 2)));
+  kern<<<grid, tc::THREADS, tc::SMEM_BYTES, s>>>(n, dofs, feat, winv, wb, r, z, zout, status);
   SFEM_CUDA(cudaGetLastError());
 }
 

@@ -1,11 +1,13 @@
 // Tensor-core (tcgen05) inference of the learned smoother's MLP, sm_100a.
 //
-// A CTA of 128 threads owns a tile of 128 cells: the MMA's M dimension.
-// Thread t builds row t of the BF16 input tile in shared memory (the
-// normalised residual of cell t plus J/h, padded 29 -> 32).  Thread 0 issues
+// A CTA runs GROUPS = 4 independent groups of 128 threads that share one
+// copy of the weights; each group owns a tile of 128 cells (the MMA's M
+// dimension), its own tensor-memory columns, mbarrier and named barrier.
+// Thread t of a group builds row t of the BF16 input tile in shared memory (the
+// normalised residual of cell t plus J/h, padded 29 -> 32).  The group's thread 0 issues
 // the tcgen05.mma instructions of each layer (BF16 operands from shared
-// memory, FP32 accumulators in tensor memory) and commits them to an
-// mbarrier.  Every thread then reads its own accumulator row back with
+// memory, FP32 accumulators in tensor memory) and commits them to the
+// group's mbarrier.  Every thread then reads its own accumulator row back with
 // tcgen05.ld, adds the bias, applies GELU (tanh form, hardware tanh) and
 // writes the BF16 activation row that feeds the next layer:
 //
@@ -40,15 +42,17 @@ namespace tc {
 constexpr int TILE = 128;       // cells per tile (MMA M)
 constexpr int K1 = 32;          // 29 inputs padded to a multiple of 16
 constexpr int N3 = 32;          // 20 outputs padded to a multiple of 16
-constexpr int TMEM_COLS = 64;   // one FP32 accumulator of up to 64 columns, reused by the layers
-constexpr int OFF_X = 0;                          // input tile  [128 x 32] bf16
-constexpr int OFF_H = OFF_X + TILE * K1 * 2;      // activations [128 x 64] bf16
-constexpr int OFF_W1 = OFF_H + TILE * 64 * 2;     // W1 [64 x 32]
+constexpr int GROUPS = 4;       // independent 128-row tile pipelines per CTA
+constexpr int THREADS = 128 * GROUPS;
+constexpr int TMEM_COLS = 64 * GROUPS;  // one 64-column FP32 accumulator per group, reused by the layers
+constexpr int XH_BYTES = TILE * 64 * 2;           // per group: input tile [128 x 32], then activations [128 x 64]
+constexpr int OFF_XH = 0;                         // GROUPS x XH_BYTES
+constexpr int OFF_W1 = OFF_XH + GROUPS * XH_BYTES; // W1 [64 x 32] (shared by the groups)
 constexpr int OFF_W2 = OFF_W1 + 64 * K1 * 2;      // W2 [64 x 64]
 constexpr int OFF_W3 = OFF_W2 + 64 * 64 * 2;      // W3 [32 x 64]
 constexpr int OFF_B = OFF_W3 + N3 * 64 * 2;       // b1[64], b2[64], b3[32] as float
-constexpr int OFF_BAR = OFF_B + 160 * 4;          // mbarrier (8 B) + tensor-memory address (4 B)
-constexpr int SMEM_BYTES = OFF_BAR + 16;
+constexpr int OFF_BAR = OFF_B + 160 * 4;          // GROUPS mbarriers (8 B each) + tensor-memory address
+constexpr int SMEM_BYTES = OFF_BAR + 8 * GROUPS + 16;
 constexpr uint32_t kWaitLimit = 1u << 24;         // polls before a wait reports a timeout
 
 __device__ __forceinline__ uint32_t smem_u32(const void* p) {
@@ -118,6 +122,19 @@ __device__ __forceinline__ void fence_async_smem() { asm volatile("fence.proxy.a
 __device__ __forceinline__ void tc_before_sync() { asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory"); }
 __device__ __forceinline__ void tc_after_sync() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }
 
+// named barrier of one 128-thread group (ids 1..GROUPS; 0 is __syncthreads)
+__device__ __forceinline__ void group_sync(int id) { asm volatile("bar.sync %0, 128;" ::"r"(id) : "memory"); }
+__device__ __forceinline__ bool group_sync_or(int id, bool v) {
+  uint32_t r;
+  asm volatile(
+      "{\n\t.reg .pred p, q;\n\tsetp.ne.u32 p, %1, 0;\n\t"
+      "bar.red.or.pred q, %2, 128, p;\n\tselp.u32 %0, 1, 0, q;\n\t}\n"
+      : "=r"(r)
+      : "r"(uint32_t(v)), "r"(id)
+      : "memory");
+  return r != 0;
+}
+
 // 8 values of one row as one 16-byte K chunk (bf16) of an R-row operand
 __device__ __forceinline__ void store_chunk(unsigned char* base, int row, int c, int R, const float* v) {
   __align__(16) __nv_bfloat162 p[4];
@@ -145,42 +162,45 @@ __device__ __forceinline__ void issue_layer(const unsigned char* smem, uint32_t 
 // (J/h and 1/h), winv [m], r in, z += correction.  MODE 1: X [n][29] in
 // (passed as feat), O [n][20] out (passed as zout); dofs/winv/r unused.
 template <int MODE, typename T>
-__global__ void __launch_bounds__(128, 4) mlp_tc_kernel(int64_t n, const int32_t* __restrict__ dofs,
-                                                        const float* __restrict__ feat,
-                                                        const float* __restrict__ winv,
-                                                        const __nv_bfloat16* __restrict__ wb,
-                                                        const T* __restrict__ r, T* __restrict__ z,
-                                                        float* __restrict__ zout, int* __restrict__ status) {
+__global__ void __launch_bounds__(tc::THREADS, 2) mlp_tc_kernel(int64_t n, const int32_t* __restrict__ dofs,
+                                                               const float* __restrict__ feat,
+                                                               const float* __restrict__ winv,
+                                                               const __nv_bfloat16* __restrict__ wb,
+                                                               const T* __restrict__ r, T* __restrict__ z,
+                                                               float* __restrict__ zout, int* __restrict__ status) {
   using D = MLPDims;
   using namespace tc;
   extern __shared__ __align__(1024) unsigned char smem[];
   float* sb = reinterpret_cast<float*>(smem + OFF_B);
   uint64_t* bar_p = reinterpret_cast<uint64_t*>(smem + OFF_BAR);
-  uint32_t* tslot = reinterpret_cast<uint32_t*>(smem + OFF_BAR + 8);
-  const int t = threadIdx.x, warp = t >> 5;
-  const uint32_t bar = smem_u32(bar_p);
+  uint32_t* tslot = reinterpret_cast<uint32_t*>(smem + OFF_BAR + 8 * GROUPS);
+  const int tid = threadIdx.x, warp = tid >> 5;
+  const int grp = tid >> 7, t = tid & 127;  // group and row within the group's tile
+  const int gbar = 1 + grp;                 // the group's named barrier
+  const uint32_t bar = smem_u32(bar_p + grp);
+  const int xh = OFF_XH + grp * XH_BYTES;   // the group's input / activation tile
 
   // weights -> shared memory (K-major, zero padding), biases as float
-  for (int i = t; i < 64 * K1; i += 128) {
+  for (int i = tid; i < 64 * K1; i += THREADS) {
     const int nn = i / K1, k = i % K1;
     const __nv_bfloat16 v = k < D::NIN ? wb[D::OFF_W1 + nn * D::NIN + k] : __float2bfloat16(0.0f);
     *reinterpret_cast<__nv_bfloat16*>(smem + OFF_W1 + kmajor_off(nn, k, 64)) = v;
   }
-  for (int i = t; i < 64 * 64; i += 128) {
+  for (int i = tid; i < 64 * 64; i += THREADS) {
     const int nn = i / 64, k = i % 64;
     *reinterpret_cast<__nv_bfloat16*>(smem + OFF_W2 + kmajor_off(nn, k, 64)) = wb[D::OFF_W2 + nn * 64 + k];
   }
-  for (int i = t; i < N3 * 64; i += 128) {
+  for (int i = tid; i < N3 * 64; i += THREADS) {
     const int nn = i / 64, k = i % 64;
     const __nv_bfloat16 v = nn < D::NOUT ? wb[D::OFF_W3 + nn * 64 + k] : __float2bfloat16(0.0f);
     *reinterpret_cast<__nv_bfloat16*>(smem + OFF_W3 + kmajor_off(nn, k, N3)) = v;
   }
-  for (int i = t; i < 160; i += 128)
+  for (int i = tid; i < 160; i += THREADS)
     sb[i] = i < 64 ? __bfloat162float(wb[D::OFF_B1 + i])
             : i < 128 ? __bfloat162float(wb[D::OFF_B2 + i - 64])
             : i < 128 + D::NOUT ? __bfloat162float(wb[D::OFF_B3 + i - 128]) : 0.0f;
-  if (t == 0) {
-    asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(bar) : "memory");
+  if (tid < GROUPS) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_u32(bar_p + tid)) : "memory");
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
   }
   if (warp == 0) {
@@ -193,13 +213,13 @@ __global__ void __launch_bounds__(128, 4) mlp_tc_kernel(int64_t n, const int32_t
   tc_before_sync();
   __syncthreads();
   tc_after_sync();
-  const uint32_t tmem = *tslot;
-  const uint32_t trow = tmem + (uint32_t(warp * 32) << 16);  // this warp's 32 accumulator lanes
+  const uint32_t tmem = *tslot + 64 * grp;                              // the group's accumulator columns
+  const uint32_t trow = tmem + (uint32_t((warp & 3) * 32) << 16);  // this warp's 32 accumulator lanes
 
   uint32_t phase = 0;
   bool failed = false;
   const int64_t n_tiles = (n + TILE - 1) / TILE;
-  for (int64_t tile = blockIdx.x; tile < n_tiles; tile += gridDim.x) {
+  for (int64_t tile = int64_t(blockIdx.x) * GROUPS + grp; tile < n_tiles; tile += int64_t(gridDim.x) * GROUPS) {
     const int64_t c = tile * TILE + t;
     const bool live = c < n;
     // ---- input row
@@ -231,29 +251,30 @@ __global__ void __launch_bounds__(128, 4) mlp_tc_kernel(int64_t n, const int32_t
       for (int i = 0; i < D::NIN; ++i) x[i] = __ldg(feat + c * D::NIN + i);
     }
 #pragma unroll
-    for (int ch = 0; ch < K1 / 8; ++ch) store_chunk(smem + OFF_X, t, ch, TILE, x + 8 * ch);
+    for (int ch = 0; ch < K1 / 8; ++ch) store_chunk(smem + xh, t, ch, TILE, x + 8 * ch);
 
-    // ---- three layers
+    // ---- three layers (the activations overwrite the input tile once the
+    // layer-1 MMAs that read it have completed)
     float v[32];
 #pragma unroll 1
     for (int layer = 0; layer < 3; ++layer) {
       fence_async_smem();
       tc_before_sync();
-      __syncthreads();
+      group_sync(gbar);
       if (t == 0) {
         tc_after_sync();
-        if (layer == 0) issue_layer(smem, tmem, OFF_X, OFF_W1, K1, 64, bar);
-        else if (layer == 1) issue_layer(smem, tmem, OFF_H, OFF_W2, 64, 64, bar);
-        else issue_layer(smem, tmem, OFF_H, OFF_W3, 64, N3, bar);
+        if (layer == 0) issue_layer(smem, tmem, xh, OFF_W1, K1, 64, bar);
+        else if (layer == 1) issue_layer(smem, tmem, xh, OFF_W2, 64, 64, bar);
+        else issue_layer(smem, tmem, xh, OFF_W3, 64, N3, bar);
       }
-      // one thread polls the mbarrier; the others wait at the block barrier
+      // one thread polls the group's mbarrier; the others wait at its barrier
       bool ok = true;
       if (t == 0) {
         ok = bar_wait(bar, phase);
         tc_before_sync();
       }
       phase ^= 1u;
-      if (__syncthreads_or(!ok)) {
+      if (group_sync_or(gbar, !ok)) {
         failed = true;
         break;
       }
@@ -274,7 +295,7 @@ __global__ void __launch_bounds__(128, 4) mlp_tc_kernel(int64_t n, const int32_t
             v[4 * q + 3] = gelu_fast(v[4 * q + 3] + bq.w);
           }
 #pragma unroll
-          for (int ch = 0; ch < 4; ++ch) store_chunk(smem + OFF_H, t, 4 * half + ch, TILE, v + 8 * ch);
+          for (int ch = 0; ch < 4; ++ch) store_chunk(smem + xh, t, 4 * half + ch, TILE, v + 8 * ch);
         }
       } else {
         tmem_ld32(trow, v);
@@ -316,7 +337,7 @@ __global__ void __launch_bounds__(128, 4) mlp_tc_kernel(int64_t n, const int32_t
   __syncthreads();
   tc_after_sync();
   if (warp == 0)
-    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(uint32_t(TMEM_COLS))
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(*tslot), "r"(uint32_t(TMEM_COLS))
                  : "memory");
 }
 
