@@ -48,6 +48,7 @@ def parse():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-solve", action="store_true", help="skip the multigrid solve measurement")
     ap.add_argument("--no-extra", action="store_true", help="skip the CG (configs 1, 1L) and batch (config 4) lines")
+    ap.add_argument("--no-learned", action="store_true", help="skip training and timing the learned smoother")
     return ap.parse_args()
 
 
@@ -198,7 +199,7 @@ def build_problem(precision):
     return mesh, op, x
 
 
-def mg_solve_bench(repeats=5):
+def mg_solve_bench(repeats=5, learned=True):
     """Poisson solve to rel. residual 1e-8: CG P3 on 64^3 x 6 tets (7,189,057 DoFs),
     f = sum of 8 sin(k.x), k ~ U[1,6]^3 (PCG64 seed 2); FP64 outer CG preconditioned by
     the hybrid p(3-2-1)/h(64-32-16-8-4) multigrid with Chebyshev(3)-Jacobi smoothing and a
@@ -228,6 +229,56 @@ def mg_solve_bench(repeats=5):
         key = "fp64_mg" if prec == "fp64" else "mixed_mg"
         out[key] = {"ms": 1e3 * min(times), "ms_median": 1e3 * statistics.median(times), "iterations": its,
                     "dofs_per_s": op.m() / min(times)}
+        del cg, mg
+    if learned:
+        # config 5: the finest-level smoother replaced by the per-cell MLP, trained
+        # here on residual/error pairs of MG-CG solves on 16^3 and 32^3 meshes
+        # (random sine loads, seeds 1000+, 200k samples), tcgen05 inference,
+        # flexible CG, Chebyshev fallback on a poor cycle
+        t0 = time.perf_counter()
+        mlp = sf.MLP(seed=1)
+        info = mlp.generate_and_train(epochs=20)
+        train_s = time.perf_counter() - t0
+        mg = sf.Multigrid(op, precision="fp32", smoother_degree=3)
+        mg.set_learned_smoother(mlp, fallback=True)
+        cg = sf.SolverCG(op, mg, flexible=True)
+        cg.solve(x, b, rtol=1e-8)
+        times = []
+        for _ in range(repeats):
+            x.zero_()
+            torch.cuda.synchronize()
+            t0 = time.perf_counter()
+            r = cg.solve(x, b, rtol=1e-8)
+            torch.cuda.synchronize()
+            times.append(time.perf_counter() - t0)
+            assert r["status"] == 0
+        out["mixed_learned_mg"] = {
+            "ms": 1e3 * min(times), "ms_median": 1e3 * statistics.median(times), "iterations": r["iterations"],
+            "fallback_iteration": r["fallback_iteration"], "dofs_per_s": op.m() / min(times),
+            "train_seconds": train_s, "train_samples": info["samples"], "loss_first": info["loss_first"],
+            "loss_last": info["loss_last"], "bounded_wait_timeouts": int(mlp.timed_out())}
+        del cg, mg
+    # DG (SIPG) P3 on 32^3 x 6 tets solved with the p/c/h multigrid (cph: CG P3
+    # right below DG P3), FP32 levels, FP64 outer CG, random load (seed 3)
+    mesh_dg = sf.Mesh(32)
+    opd = sf.Operator(mesh_dg, 3, "dg", "fp64")
+    bd = torch.tensor(__import__("numpy").random.default_rng(3).uniform(-1, 1, opd.m()), device="cuda")
+    xd = opd.initialize_dof_vector()
+    for ct, name in ((0, "dg_mg_phc"), (1, "dg_mg_cph")):
+        mg = sf.Multigrid(opd, precision="fp32", smoother_degree=3, c_transfer=ct)
+        cg = sf.SolverCG(opd, mg)
+        cg.solve(xd, bd, rtol=1e-8)
+        times = []
+        for _ in range(repeats):
+            xd.zero_()
+            torch.cuda.synchronize()
+            t0 = time.perf_counter()
+            r = cg.solve(xd, bd, rtol=1e-8)
+            torch.cuda.synchronize()
+            times.append(time.perf_counter() - t0)
+            assert r["status"] == 0
+        out[name] = {"workload": "DG SIPG P3, 32^3 x 6 tets (3,932,160 DoFs), mixed MG-CG to 1e-8",
+                     "ms": 1e3 * min(times), "iterations": r["iterations"]}
         del cg, mg
     return out
 
@@ -463,7 +514,7 @@ def run_ours(args):
     achieved_gbs = alg_bytes / (apply_ms / 1e3) / 1e9
     vm_ms = statistics.mean(t64)
     fp64_peak = fp64_peak_tflops() if rank == 0 else None
-    solve = mg_solve_bench() if (rank == 0 and not args.no_solve) else None
+    solve = mg_solve_bench(learned=not args.no_learned) if (rank == 0 and not args.no_solve) else None
     extra_cfg = None
     if rank == 0 and not args.no_extra:
         extra_cfg = cg_vmult_bench(min(args.steps, 100), 3, flush)
