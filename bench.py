@@ -49,6 +49,8 @@ def parse():
     ap.add_argument("--no-solve", action="store_true", help="skip the multigrid solve measurement")
     ap.add_argument("--no-extra", action="store_true", help="skip the CG (configs 1, 1L) and batch (config 4) lines")
     ap.add_argument("--no-learned", action="store_true", help="skip training and timing the learned smoother")
+    ap.add_argument("--case", choices=["cg-p2-64", "cg-p1-128", "cg-p2-128", "mlp-64"],
+                    help="run one small kernel workload (for profiling) instead of the benchmark")
     return ap.parse_args()
 
 
@@ -555,8 +557,49 @@ def run_ours(args):
         dist.destroy_process_group()
 
 
+def run_case(name, reps=3):
+    """One small workload of a single kernel family, for profiling (ncu -k ...):
+    cg-p2-64 / cg-p1-128 / cg-p2-128: CG vmults (default kernel variant, FP64 and
+    FP32) on 64^3 or 128^3 x 6 tets, jitter 0.1h; mlp-64: eager V-cycles of the
+    mixed multigrid with the learned finest-level smoother on CG P3 64^3
+    (untrained network: the kernels do the same work)."""
+    import torch
+    import simplexfem as sf
+    out = {"case": name}
+    if name.startswith("cg-"):
+        p, n = int(name[4]), int(name.split("-")[2])
+        mesh = sf.Mesh(n, jitter=JITTER, seed=0)
+        for prec in ("fp64", "fp32"):
+            op = sf.Operator(mesh, p, "cg", prec)
+            x = torch.rand(op.m(), dtype=op.dtype, device="cuda")
+            y = op.initialize_dof_vector()
+            for _ in range(reps):
+                op.vmult(y, x)
+            torch.cuda.synchronize()
+            out[prec] = {"m": op.m(), "finite": bool(torch.isfinite(y).all())}
+    elif name == "mlp-64":
+        mesh = sf.Mesh(64)
+        op = sf.Operator(mesh, 3, "cg", "fp64")
+        mg = sf.Multigrid(op, precision="fp32", use_graph=False)
+        mlp = sf.MLP(seed=1)
+        mg.set_learned_smoother(mlp, fallback=False)
+        b = torch.rand(op.m(), dtype=torch.float64, device="cuda")
+        x = op.initialize_dof_vector()
+        for _ in range(reps):
+            mg.vmult(x, b)
+        torch.cuda.synchronize()
+        out["finite"] = bool(torch.isfinite(x).all())
+        out["timed_out"] = mlp.timed_out()
+    else:
+        raise SystemExit(f"unknown case {name}")
+    print(json.dumps(out), flush=True)
+
+
 def main():
     args = parse()
+    if args.case:
+        run_case(args.case)
+        return
     if args.impl == "reference":
         run_reference(args)
     else:
