@@ -315,9 +315,16 @@ class CGOperator final : public Operator {
       return;
     }
     // default (variant 0), measured on B200: P1 per hex, P2 per cube, P3 per
-    // cube in FP32 and per cell in FP64
+    // cube in FP32 and per cell in FP64; per cell on meshes too small to give
+    // every SM two cubes (or two CTAs of hexes), where the coarser forms
+    // leave SMs idle
     int v = cfg.kernel_variant;
-    if (v == 0) v = cfg.degree == 1 ? 2 : cfg.degree == 2 ? 3 : (sizeof(T) == 4 ? 3 : 1);
+    if (v == 0) {
+      constexpr int64_t kFill = 2 * 148;
+      v = cfg.degree == 1 ? 2 : cfg.degree == 2 ? 3 : (sizeof(T) == 4 ? 3 : 1);
+      if (v == 3 && n_blocks < kFill) v = 2;
+      if (v == 2 && n_hex < kFill * kHexBS) v = 1;
+    }
     if (v == 3 && cube_NB) {
       switch (cfg.degree) {
         case 1: launch_cube<1, 125, 5>(x, d, s); break;
