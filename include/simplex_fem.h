@@ -85,7 +85,10 @@ typedef struct fem_op_params {
                               cell, 2 thread per Kuhn hex (6 tets, one atomic per distinct
                               DoF), 3 CTA per 4x4x4-hex Morton cube (stores for cube-interior
                               DoFs); each falls back to the next simpler form where the mesh
-                              lacks the pattern; default P1 2, P2 3, P3 3 (FP32) / 1 (FP64) */
+                              lacks the pattern; default P1 2, P2 3, P3 3 (FP32) / 1 (FP64);
+                              4: FP32 CG on the TF32 tensor cores (tcgen05 kind::tf32, cell
+                              operator as one [128 cells x K] x [K x 6K] product; ~1e-3
+                              relative accuracy, for multigrid levels) */
   int32_t reserved[5];
 } fem_op_params;
 
@@ -164,6 +167,11 @@ int fem_op_vmult_phase(fem_op* op, void* dst, const void* src, int32_t phase, vo
 int fem_op_set_kernel_variant(fem_op* op, int32_t variant);
 /* Algorithmic work of one vmult: flops and bytes of the fused kernels. */
 int fem_op_work(const fem_op* op, double* flops, double* bytes);
+/* Device-side status of the operator's kernels since the last call, then
+ * cleared: bit 0 = a tensor-core kernel gave up on a bounded wait (that
+ * vmult's result is invalid).  Synchronises with the device.  No counterpart
+ * in the reference (its kernels have no bounded waits). */
+int fem_op_status(fem_op* op, int32_t* status);
 
 /* ---- loads --------------------------------------------------------------
  * f(x) = sum_m amp[m] sin(k[m] . x)           (kind FEM_RHS_PLANE_WAVES)
@@ -204,7 +212,9 @@ typedef struct fem_mg_params {
                                1 = CG P_p right below DG P_p, then the CG ladder of `order`
                                (cph / chp; DG/cells_batched/application_phc.cc:3396-3652) */
   int32_t learned_steps;    /* learned finest-level smoothing per V-cycle: 1 pre, 2 post, 3 both (3) */
-  int32_t reserved[2];
+  int32_t tensor_cores;     /* FP32 CG levels apply their operator with TF32 tensor-core
+                               contractions (kernel variant 4; operator accurate to ~1e-3) */
+  int32_t reserved[1];
 } fem_mg_params;
 int fem_mg_params_default(fem_mg_params* p);
 int fem_mg_create(fem_op* fine, const fem_mg_params* p, fem_mg** out);

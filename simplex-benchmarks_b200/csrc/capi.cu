@@ -124,7 +124,7 @@ int fem_op_create(fem_mesh* mesh, int32_t degree, int32_t kind, int32_t precisio
       }
       cfg.penalty = params->penalty;
       cfg.kernel_variant = params->kernel_variant;
-      SFEM_REQUIRE(cfg.kernel_variant >= 0 && cfg.kernel_variant <= 3, FEM_ERR_ARG, "kernel_variant must be 0..3");
+      SFEM_REQUIRE(cfg.kernel_variant >= 0 && cfg.kernel_variant <= 4, FEM_ERR_ARG, "kernel_variant must be 0..4");
       SFEM_REQUIRE(cfg.penalty == FEM_PENALTY_REFERENCE || cfg.penalty == FEM_PENALTY_SQUARE, FEM_ERR_ARG,
                    "penalty must be FEM_PENALTY_REFERENCE or FEM_PENALTY_SQUARE");
     }
@@ -234,7 +234,9 @@ int fem_op_compute_diagonal(fem_op* op, void* diag, void* stream) {
 int fem_op_set_kernel_variant(fem_op* op, int32_t variant) {
   return guarded([&] {
     REQUIRE_PTR(op);
-    SFEM_REQUIRE(variant >= 0 && variant <= 3, FEM_ERR_ARG, "kernel_variant must be 0..3");
+    SFEM_REQUIRE(variant >= 0 && variant <= 4, FEM_ERR_ARG, "kernel_variant must be 0..4");
+    SFEM_REQUIRE(variant != 4 || (op->op->cfg.kind == FEM_CG && op->op->cfg.precision == FEM_FP32), FEM_ERR_ARG,
+                 "kernel_variant 4 (TF32 tensor cores) is for FP32 CG operators");
     op->op->cfg.kernel_variant = variant;
   });
 }
@@ -246,6 +248,14 @@ int fem_op_work(const fem_op* op, double* flops, double* bytes) {
     op->op->work(f, b);
     if (flops) *flops = f;
     if (bytes) *bytes = b;
+  });
+}
+
+int fem_op_status(fem_op* op, int32_t* status) {
+  return guarded([&] {
+    REQUIRE_PTR(op);
+    REQUIRE_PTR(status);
+    *status = op->op->status(true);
   });
 }
 

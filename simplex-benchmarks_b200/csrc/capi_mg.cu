@@ -82,6 +82,7 @@ int fem_mg_params_default(fem_mg_params* p) {
     p->use_graph = d.use_graph;
     p->c_transfer = d.c_transfer;
     p->learned_steps = d.learned_steps;
+    p->tensor_cores = d.tensor_cores;
   });
 }
 
@@ -101,6 +102,7 @@ int fem_mg_create(fem_op* fine, const fem_mg_params* p, fem_mg** out) {
       prm.use_graph = p->use_graph;
       prm.c_transfer = p->c_transfer;
       prm.learned_steps = p->learned_steps;
+      prm.tensor_cores = p->tensor_cores;
     }
     SFEM_REQUIRE(prm.learned_steps >= 1 && prm.learned_steps <= 3, FEM_ERR_ARG, "mg: learned_steps must be 1..3");
     SFEM_REQUIRE(prm.order == FEM_MG_PH || prm.order == FEM_MG_HP, FEM_ERR_ARG, "mg: order must be PH or HP");

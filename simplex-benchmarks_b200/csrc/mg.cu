@@ -459,6 +459,7 @@ class MultigridImpl final : public Multigrid {
       L.hexes = L.mesh->desc.n[0];
       cfg.degree = L.degree;
       cfg.kind = L.kind;
+      cfg.kernel_variant = prm.tensor_cores && L.kind == FEM_CG && cfg.precision == FEM_FP32 ? 4 : 0;
       L.op = make_operator(*L.mesh, cfg);
       const int64_t m = L.op->m;
       L.inv_diag.alloc(m);
@@ -601,6 +602,7 @@ class MultigridImpl final : public Multigrid {
     const Level& L0 = levels_[0];
     OpConfig cfg = L0.op->cfg;
     cfg.precision = FEM_FP64;
+    cfg.kernel_variant = 0;
     auto op64 = make_operator(*L0.mesh, cfg);
     const int n = int(op64->m);
     SFEM_REQUIRE(n <= 8192, FEM_ERR_ARG, "multigrid: coarse level too large for the dense solve");

@@ -32,6 +32,9 @@ struct MGParams {
   int c_transfer = 0;
   // finest-level learned smoothing steps per V-cycle: 1 pre, 2 post, 3 both
   int learned_steps = 3;
+  // FP32 CG levels apply their operator on the TF32 tensor cores
+  // (cg_cell_tc_kernel, kernel variant 4)
+  int tensor_cores = 0;
 };
 
 class Multigrid {

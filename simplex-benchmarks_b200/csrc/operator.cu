@@ -5,6 +5,7 @@
 #include <unordered_map>
 
 #include "kernels_cg.cuh"
+#include "kernels_cg_tc.cuh"
 #include "kernels_dg.cuh"
 #include "kernels_dg3.cuh"
 #include "autotune.hpp"
@@ -69,6 +70,56 @@ class CGOperator final : public Operator {
   int hex_H = 0;
 
   static int hex_dofs(int p) { return p == 1 ? 8 : p == 2 ? 27 : 64; }
+
+  // TF32 tensor-core tables (variant 4, FP32 operators): B = [S_0; ..; S_5]
+  DevBuf<float> d_btc;
+  DevBuf<int> d_status;
+  int tc_grid = 0;
+
+  template <int P>
+  void build_tc_tables() {
+    using Tb = ref::Tables<P>;
+    using Sh = CGTcShape<P>;
+    constexpr int KQ = Tb::KQ;
+    // E_ab = D_a^T MQ D_b, [K][K]
+    auto E = [&](int a, int b, int i, int j) {
+      double s = 0;
+      for (int m = 0; m < KQ; ++m)
+        for (int q = 0; q < KQ; ++q) s += Tb::D[a][m][i] * Tb::MQ[m][q] * Tb::D[b][q][j];
+      return s;
+    };
+    static const int ca[6] = {0, 1, 2, 0, 0, 1}, cb[6] = {0, 1, 2, 1, 2, 2};
+    std::vector<float> B(size_t(Sh::NPAD) * Sh::KPAD, 0.0f);
+    for (int c = 0; c < 6; ++c)
+      for (int i = 0; i < Sh::K; ++i)
+        for (int j = 0; j < Sh::K; ++j) {
+          double v = E(ca[c], cb[c], i, j);
+          if (ca[c] != cb[c]) v += E(cb[c], ca[c], i, j);
+          // round to TF32 (10 mantissa bits, nearest, ties away)
+          float f = float(v);
+          uint32_t bits;
+          std::memcpy(&bits, &f, 4);
+          bits = (bits + 0x1000u) & 0xFFFFE000u;
+          std::memcpy(&f, &bits, 4);
+          B[size_t(c * Sh::K + i) * Sh::KPAD + j] = f;
+        }
+    d_btc.upload(B);
+    int dev = 0, sms = 0, occ = 0;
+    SFEM_CUDA(cudaGetDevice(&dev));
+    SFEM_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+    SFEM_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, cg_cell_tc_kernel<P>, 128, Sh::SMEM_BYTES));
+    occ = std::min(occ, 512 / Sh::TMEM_COLS);  // tensor-memory columns per SM
+    SFEM_REQUIRE(occ > 0, FEM_ERR_CUDA, "CG tensor-core kernel does not fit on an SM");
+    tc_grid = int(std::min<int64_t>((n_cells + 127) / 128, int64_t(sms) * occ));
+  }
+
+  int status(bool clear) override {
+    if (!d_status.p) return 0;
+    int v = 0;
+    SFEM_CUDA(cudaMemcpy(&v, d_status.p, sizeof(int), cudaMemcpyDeviceToHost));
+    if (clear && v) SFEM_CUDA(cudaMemset(d_status.p, 0, sizeof(int)));
+    return v;
+  }
 
   // cube-block tables of cg_cube_kernel (blocks of 64 hexes = 384 tets)
   DevBuf<int16_t> d_tmap, d_rptr, d_rdof, d_cptr, d_cslot;
@@ -167,6 +218,17 @@ class CGOperator final : public Operator {
     d_bdof.upload(bd);
     n_blocks = nbk;
     cube_NB = NB;
+  }
+
+  void launch_tc_cell(const T* x, T* d, cudaStream_t s) {
+    const float* xf = reinterpret_cast<const float*>(x);
+    float* df = reinterpret_cast<float*>(d);
+    switch (cfg.degree) {
+      case 1: cg_cell_tc_kernel<1><<<tc_grid, 128, CGTcShape<1>::SMEM_BYTES, s>>>(n_cells, d_dofs.p, reinterpret_cast<const float*>(d_geo.p), d_btc.p, xf, df, d_constrained.n, d_constrained.p, d_status.p); break;
+      case 2: cg_cell_tc_kernel<2><<<tc_grid, 128, CGTcShape<2>::SMEM_BYTES, s>>>(n_cells, d_dofs.p, reinterpret_cast<const float*>(d_geo.p), d_btc.p, xf, df, d_constrained.n, d_constrained.p, d_status.p); break;
+      case 3: cg_cell_tc_kernel<3><<<tc_grid, 128, CGTcShape<3>::SMEM_BYTES, s>>>(n_cells, d_dofs.p, reinterpret_cast<const float*>(d_geo.p), d_btc.p, xf, df, d_constrained.n, d_constrained.p, d_status.p); break;
+    }
+    SFEM_CUDA(cudaGetLastError());
   }
 
   template <int P, int NB, int KP>
@@ -271,6 +333,15 @@ class CGOperator final : public Operator {
     d_constrained.upload(cl);
     build_hex_tables(mesh, dofs, geo);
     build_cube_tables(dofs);
+    d_status.alloc(1);
+    SFEM_CUDA(cudaMemset(d_status.p, 0, sizeof(int)));
+    if (std::is_same<T, float>::value && n_cells > 0) {
+      switch (cfg.degree) {
+        case 1: build_tc_tables<1>(); break;
+        case 2: build_tc_tables<2>(); break;
+        case 3: build_tc_tables<3>(); break;
+      }
+    }
     if (cube_NB) {
       switch (cfg.degree) {
         case 1: setup_cube<1, 125, 5>(); break;
@@ -319,6 +390,11 @@ class CGOperator final : public Operator {
     // every SM two cubes (or two CTAs of hexes), where the coarser forms
     // leave SMs idle
     int v = cfg.kernel_variant;
+    if (v == 4) {
+      SFEM_REQUIRE(d_btc.p != nullptr, FEM_ERR_ARG, "CG kernel variant 4 (TF32 tensor cores) needs an FP32 operator");
+      launch_tc_cell(x, d, s);
+      return;
+    }
     if (v == 0) {
       constexpr int64_t kFill = 2 * 148;
       v = cfg.degree == 1 ? 2 : cfg.degree == 2 ? 3 : (sizeof(T) == 4 ? 3 : 1);

@@ -91,6 +91,9 @@ class Operator {
     throw Error(FEM_ERR_ARG, "this operator kind uses no scratch memory");
   }
   void inverse_diagonal(void* diag, cudaStream_t s);
+  // device-side status bits of the operator's kernels since the last call
+  // (bit 0: a tensor-core kernel gave up on a bounded wait); clear resets them
+  virtual int status(bool clear) { return 0; }
   // flops of the fused kernels and algorithmic bytes (src+dst once, index and
   // geometry data once) of one vmult
   virtual void work(double& flops, double& bytes) const = 0;

@@ -49,7 +49,7 @@ class MGParams(C.Structure):
     _fields_ = [("order", C.c_int32), ("precision", C.c_int32), ("smoother_degree", C.c_int32),
                 ("eig_iterations", C.c_int32), ("smoothing_range", C.c_double), ("eig_safety", C.c_double),
                 ("coarse_n", C.c_int32), ("use_graph", C.c_int32), ("c_transfer", C.c_int32),
-                ("learned_steps", C.c_int32), ("reserved", C.c_int32 * 2)]
+                ("learned_steps", C.c_int32), ("tensor_cores", C.c_int32), ("reserved", C.c_int32 * 1)]
 
 
 class SolveInfo(C.Structure):
@@ -104,6 +104,7 @@ _PROTOS = [
     ("fem_op_compute_diagonal", C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p]),
     ("fem_op_set_kernel_variant", C.c_int, [C.c_void_p, C.c_int32]),
     ("fem_op_work", C.c_int, [C.c_void_p, C.POINTER(C.c_double), C.POINTER(C.c_double)]),
+    ("fem_op_status", C.c_int, [C.c_void_p, C.POINTER(C.c_int32)]),
     ("fem_op_rhs", C.c_int, [C.c_void_p, C.POINTER(RhsDesc), C.c_void_p, C.c_void_p]),
     ("fem_op_interpolate", C.c_int, [C.c_void_p, C.POINTER(RhsDesc), C.c_void_p, C.c_void_p]),
     ("fem_mg_params_default", C.c_int, [C.POINTER(MGParams)]),
@@ -316,6 +317,12 @@ class Operator:
     def set_kernel_variant(self, variant):
         check(lib().fem_op_set_kernel_variant(self.handle, variant))
 
+    def status(self):
+        """Device-side status bits since the last call (0: every bounded wait completed)."""
+        v = C.c_int32()
+        check(lib().fem_op_status(self.handle, C.byref(v)))
+        return v.value
+
     def autotune(self, reps=20, use_cache=True):
         """Time the kernel variants on this operator and keep the fastest
         (fem_op_autotune); returns {"variant", "cached", "us": [per variant]}."""
@@ -412,7 +419,8 @@ class Multigrid:
     c_transfer=1 hands over at P_p (cph with FEM_MG_PH, chp with FEM_MG_HP)."""
 
     def __init__(self, fine_op, order=FEM_MG_PH, precision="fp32", smoother_degree=3, smoothing_range=20.0,
-                 eig_iterations=10, eig_safety=1.2, coarse_n=4, use_graph=True, c_transfer=0, learned_steps=3):
+                 eig_iterations=10, eig_safety=1.2, coarse_n=4, use_graph=True, c_transfer=0, learned_steps=3,
+                 tensor_cores=False):
         p = MGParams()
         check(lib().fem_mg_params_default(C.byref(p)))
         p.order = order
@@ -425,6 +433,7 @@ class Multigrid:
         p.use_graph = int(bool(use_graph))
         p.c_transfer = c_transfer
         p.learned_steps = learned_steps
+        p.tensor_cores = int(bool(tensor_cores))
         h = C.c_void_p()
         check(lib().fem_mg_create(fine_op.handle, C.byref(p), C.byref(h)))
         self.handle = h

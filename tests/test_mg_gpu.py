@@ -203,3 +203,20 @@ def test_dg_multigrid_iterations_match_oracle(cuda, p, c_transfer, order):
     assert abs(res["iterations"] - its) <= 1, (res["iterations"], its)
     xs = x.cpu().numpy()
     assert np.linalg.norm(top.A @ xs - bh) <= 1.1e-8 * np.linalg.norm(bh)
+
+
+def test_mg_with_tf32_tensor_core_levels(cuda):
+    """Mixed multigrid whose FP32 CG levels run on the TF32 tensor cores reaches
+    1e-8 (the outer CG stays FP64) within 2 iterations of the CUDA-core levels."""
+    import torch
+    mesh = sf.Mesh(16)
+    op = sf.Operator(mesh, 3, "cg")
+    b = sf.rhs(op, sf.sine_modes_rhs())
+    its = {}
+    for tc in (False, True):
+        mg = sf.Multigrid(op, precision="fp32", tensor_cores=tc)
+        x = op.initialize_dof_vector()
+        r = sf.SolverCG(op, mg).solve(x, b, rtol=1e-8, max_iterations=100)
+        assert r["status"] == sf.FEM_OK, r
+        its[tc] = r["iterations"]
+    assert its[True] <= its[False] + 2, its
