@@ -235,8 +235,8 @@ int fem_op_set_kernel_variant(fem_op* op, int32_t variant) {
   return guarded([&] {
     REQUIRE_PTR(op);
     SFEM_REQUIRE(variant >= 0 && variant <= 4, FEM_ERR_ARG, "kernel_variant must be 0..4");
-    SFEM_REQUIRE(variant != 4 || (op->op->cfg.kind == FEM_CG && op->op->cfg.precision == FEM_FP32), FEM_ERR_ARG,
-                 "kernel_variant 4 (TF32 tensor cores) is for FP32 CG operators");
+    SFEM_REQUIRE(variant != 4 || op->op->cfg.kind != FEM_CG || op->op->cfg.precision == FEM_FP32, FEM_ERR_ARG,
+                 "CG kernel_variant 4 (TF32 tensor cores) is for FP32 operators");
     op->op->cfg.kernel_variant = variant;
   });
 }
@@ -286,7 +286,7 @@ int fem_op_autotune(fem_op* op, int32_t reps, int32_t use_cache, int32_t* varian
     if (variant) *variant = r.variant;
     if (cached) *cached = r.cached ? 1 : 0;
     if (us)
-      for (int i = 0; i < 3; ++i) us[i] = i < int(r.us.size()) ? r.us[i] : 0.0;
+      for (int i = 0; i < 4; ++i) us[i] = i < int(r.us.size()) ? r.us[i] : 0.0;
   });
 }
 
@@ -298,7 +298,7 @@ int fem_batch_autotune(fem_batch* batch, int32_t reps, int32_t use_cache, int32_
     if (variant) *variant = r.variant;
     if (cached) *cached = r.cached ? 1 : 0;
     if (us)
-      for (int i = 0; i < 3; ++i) us[i] = i < int(r.us.size()) ? r.us[i] : 0.0;
+      for (int i = 0; i < 4; ++i) us[i] = i < int(r.us.size()) ? r.us[i] : 0.0;
   });
 }
 

@@ -277,15 +277,20 @@ __device__ __forceinline__ void load_cell(const DGProblem<T>& pr, int64_t c, Cel
   }
 }
 
-template <int P, int NC, bool MASS, int BS, typename T>
-__global__ void __launch_bounds__(BS, BS == 64 ? 6 : 1) dg_apply_kernel(const __grid_constant__ DGBatch<T> batch,
-                                                                       int64_t n_blocks) {
+// MINB: minimum resident CTAs per SM (register cap).  ALIAS (NC == 1): the
+// results stay in registers until every thread of the CTA is done reading the
+// staged src rows, then reuse those rows for the coalesced write-out, so the
+// CTA needs no separate result rows (less shared memory, more CTAs per SM).
+template <int P, int NC, bool MASS, int BS, typename T, int MINB = (BS == 64 ? 6 : 1), bool ALIAS = false>
+__global__ void __launch_bounds__(BS, MINB) dg_apply_kernel(const __grid_constant__ DGBatch<T> batch,
+                                                            int64_t n_blocks) {
   using O = gen::Ops<P>;
   using S = DGShape<P, NC>;
+  static_assert(!ALIAS || NC == 1, "result aliasing holds one component in registers");
   extern __shared__ __align__(16) unsigned char smem_raw[];
   T* su = reinterpret_cast<T*>(smem_raw);  // [BS][US]  src rows
   T* sq = su + BS * S::US;                 // [BS][QS]  published traces
-  T* sy = sq + BS * S::QS;                 // [BS][US]  results
+  T* sy = ALIAS ? su : sq + BS * S::QS;    // [BS][US]  results
   for (int64_t blk = blockIdx.x; blk < n_blocks; blk += gridDim.x) {
     const int pi = find_problem(batch, blk);
     const DGProblem<T>& pr = batch.p[pi];
@@ -296,7 +301,20 @@ __global__ void __launch_bounds__(BS, BS == 64 ? 6 : 1) dg_apply_kernel(const __
     stage_in<S::QN, S::QS, BS>(sq, pr.Q + c0 * S::QN, nloc);
     __syncthreads();
     const int t = threadIdx.x;
-    if (t < nloc) {
+    if (ALIAS) {
+      T y[O::K];
+      if (t < nloc) {
+        CellData<T> d;
+        load_cell<MASS>(pr, c0 + t, d);
+        dg_cell_component<P, NC, MASS, true>(pr, c0, 0, su + t * S::US, sq + t * S::QS, su, sq, nloc, d.G, d.sf,
+                                             d.md, d.nb, d.nbf, y);
+      }
+      __syncthreads();  // every thread is done with the staged src rows
+      if (t < nloc) {
+#pragma unroll
+        for (int i = 0; i < O::K; ++i) sy[t * S::US + i] = y[i];
+      }
+    } else if (t < nloc) {
       CellData<T> d;
       load_cell<MASS>(pr, c0 + t, d);
 #pragma unroll 1

@@ -637,18 +637,19 @@ class DGOperator final : public Operator {
     }
   }
 
-  template <int P, int NC, bool MASS, int BS>
+  template <int P, int NC, bool MASS, int BS, int MINB = (BS == 64 ? 6 : 1), bool ALIAS = false>
   static void run_cell(const DGProblem<T>* probs, int n, cudaStream_t s, int what) {
     using S = DGShape<P, NC>;
     int64_t n_blocks = 0;
     const DGBatch<T> b = make_batch(probs, n, BS, n_blocks);
     const size_t sm_trace = size_t(BS) * (S::US + S::QS) * sizeof(T);
-    const size_t sm_apply = size_t(BS) * (2 * S::US + S::QS) * sizeof(T);
+    const size_t sm_apply = size_t(BS) * ((ALIAS ? 1 : 2) * S::US + S::QS) * sizeof(T);
     static int conf_t = 0, conf_a = 0;
+    auto apply = dg_apply_kernel<P, NC, MASS, BS, T, MINB, ALIAS>;
     opt_in_smem(dg_trace_kernel<P, NC, BS, T>, sm_trace, conf_t);
-    opt_in_smem(dg_apply_kernel<P, NC, MASS, BS, T>, sm_apply, conf_a);
+    opt_in_smem(apply, sm_apply, conf_a);
     if (what != 2) dg_trace_kernel<P, NC, BS, T><<<unsigned(n_blocks), BS, sm_trace, s>>>(b, n_blocks);
-    if (what != 1) dg_apply_kernel<P, NC, MASS, BS, T><<<unsigned(n_blocks), BS, sm_apply, s>>>(b, n_blocks);
+    if (what != 1) apply<<<unsigned(n_blocks), BS, sm_apply, s>>>(b, n_blocks);
   }
 
   template <int P, int NC, bool MASS>
@@ -677,8 +678,13 @@ class DGOperator final : public Operator {
       run_cell<P, NC, MASS, 64>(probs, n, s, what);
     } else if (variant == 3) {
       run_warp<P, NC, MASS>(probs, n, s, what);
+    } else if (variant == 4) {
+      // 64 cells per CTA, results aliased onto the staged src rows (scalar
+      // problems), registers capped for 8 CTAs per SM
+      if (NC == 1) run_cell<P, NC, MASS, 64, 8, (NC == 1)>(probs, n, s, what);
+      else run_cell<P, NC, MASS, 64, 8, false>(probs, n, s, what);
     } else {
-      throw Error(FEM_ERR_ARG, "DG: kernel variant must be 0..3");
+      throw Error(FEM_ERR_ARG, "DG: kernel variant must be 0..4");
     }
     SFEM_CUDA(cudaGetLastError());
   }
@@ -708,12 +714,12 @@ class DGBatchImpl final : public Batch {
   }
   int variant() const override { return cfg.kernel_variant; }
   void set_variant(int v) override {
-    SFEM_REQUIRE(v >= 0 && v <= 3, FEM_ERR_ARG, "batch: kernel variant must be 0..3");
+    SFEM_REQUIRE(v >= 0 && v <= 4, FEM_ERR_ARG, "batch: kernel variant must be 0..4");
     cfg.kernel_variant = v;
   }
   TuneResult tune(int reps, bool use_cache) override {
     TuneResult res;
-    res.us.assign(3, 0.0);
+    res.us.assign(4, 0.0);
     int64_t cells = 0;
     for (auto* o : ops) cells += o->n_cells;
     const std::string key = "batch" + std::to_string(ops.size()) + "," + tune_key(cfg, cells);

@@ -236,3 +236,17 @@ def test_cg_tf32_tensor_core_variant(cuda, p):
     assert rel_l2(y, ref) <= 3e-3
     with pytest.raises(sf.FemError):
         sf.Operator(mesh, p, "cg", "fp64").set_kernel_variant(4)
+
+
+@pytest.mark.parametrize("variant", [1, 2, 3, 4])
+@pytest.mark.parametrize("kind", ["dg", "helmholtz"])
+@pytest.mark.parametrize("p", [1, 2, 3])
+def test_dg_kernel_variants(cuda, p, kind, variant):
+    """Every DG / Helmholtz kernel shape (the autotuner's candidates) against the oracle, FP64."""
+    mesh = sf.Mesh((5, 4, 3), jitter=0.1, seed=2)
+    op = sf.Operator(mesh, p, kind, "fp64")
+    op.set_kernel_variant(variant)
+    x = seeded_src(op.m(), 4)
+    y = run_product(op, x)
+    ref = orc.for_mesh(mesh, p, KIND[kind], n_components=op.n_components).vmult(x)
+    assert rel_l2(y, ref) <= 1e-12
