@@ -54,6 +54,18 @@ def parse():
     return ap.parse_args()
 
 
+def max_over_ranks(value, device):
+    """The largest `value` over the ranks of the default process group (the
+    timed region ends when the slowest rank ends); the value itself without one."""
+    import torch
+    import torch.distributed as dist
+    if not dist.is_available() or not dist.is_initialized() or dist.get_world_size() == 1:
+        return value
+    t = torch.tensor([float(value)], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
 def dist_env():
     return int(os.environ.get("RANK", 0)), int(os.environ.get("WORLD_SIZE", 1)), int(os.environ.get("LOCAL_RANK", 0))
 
@@ -469,11 +481,7 @@ def run_ours(args):
     with ClockSampler(local) as clk:
         t64 = timed_steps(lambda: op.vmult(dst, src, stream), args.steps, args.warmup, stream, flush)
     barrier()
-    total_ms = sum(t64)
-    if world > 1:
-        t = torch.tensor([total_ms], device="cuda", dtype=torch.float64)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        total_ms = float(t.item())
+    total_ms = max_over_ranks(sum(t64), "cuda")
     value = op.m() * args.steps * world / (total_ms / 1e3)
 
     # ---- per-kernel times (dominant kernel for the roofline)
@@ -498,11 +506,7 @@ def run_ours(args):
             hdst.copy_(dst, non_blocking=True)
 
     te2e = timed_steps(e2e_step, args.steps, args.warmup, stream, None)
-    e2e_ms = sum(te2e)
-    if world > 1:
-        t = torch.tensor([e2e_ms], device="cuda", dtype=torch.float64)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        e2e_ms = float(t.item())
+    e2e_ms = max_over_ranks(sum(te2e), "cuda")
     e2e_value = op.m() * args.steps * world / (e2e_ms / 1e3)
     nbytes = op.m() * 8
 
