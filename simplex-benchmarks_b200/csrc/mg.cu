@@ -97,6 +97,74 @@ __global__ void transfer_restrict_add(int64_t nf, int Kf, int Kc, const int32_t*
   }
 }
 
+// The same two transfers with the local matrix shape known at compile time
+// (every p and h pair of the ladders): fully unrolled loops over registers.
+template <typename T, int KF, int KC>
+__global__ void __launch_bounds__(128) transfer_prolongate_add_k(int64_t nf, const int32_t* __restrict__ parent,
+                                                                 const uint8_t* __restrict__ mid,
+                                                                 const uint32_t* __restrict__ owner,
+                                                                 const double* __restrict__ mats,
+                                                                 const int32_t* __restrict__ fdofs,
+                                                                 const int32_t* __restrict__ cdofs, int64_t nc,
+                                                                 const T* __restrict__ xc, T* __restrict__ xf) {
+  const int64_t c = blockIdx.x * int64_t(blockDim.x) + threadIdx.x;
+  if (c >= nf) return;
+  const uint32_t ow = __ldg(owner + c);
+  if (!ow) return;
+  const int64_t pc = __ldg(parent + c);
+  const double* M = mats + int64_t(__ldg(mid + c)) * KF * KC;
+  double xl[KC];
+#pragma unroll
+  for (int j = 0; j < KC; ++j) {
+    const int32_t g = __ldg(cdofs + j * nc + pc);
+    xl[j] = g >= 0 ? double(__ldg(xc + g)) : 0.0;
+  }
+#pragma unroll
+  for (int i = 0; i < KF; ++i) {
+    if (!((ow >> i) & 1u)) continue;
+    const int32_t g = __ldg(fdofs + i * nf + c);
+    if (g < 0) continue;
+    double acc = 0.0;
+#pragma unroll
+    for (int j = 0; j < KC; ++j) acc += __ldg(M + i * KC + j) * xl[j];
+    xf[g] += T(acc);
+  }
+}
+
+template <typename T, int KF, int KC>
+__global__ void __launch_bounds__(128) transfer_restrict_add_k(int64_t nf, const int32_t* __restrict__ parent,
+                                                               const uint8_t* __restrict__ mid,
+                                                               const uint32_t* __restrict__ owner,
+                                                               const double* __restrict__ mats,
+                                                               const int32_t* __restrict__ fdofs,
+                                                               const int32_t* __restrict__ cdofs, int64_t nc,
+                                                               const T* __restrict__ xf, T* __restrict__ xc) {
+  const int64_t c = blockIdx.x * int64_t(blockDim.x) + threadIdx.x;
+  if (c >= nf) return;
+  const uint32_t ow = __ldg(owner + c);
+  if (!ow) return;
+  const int64_t pc = __ldg(parent + c);
+  const double* M = mats + int64_t(__ldg(mid + c)) * KF * KC;
+  double rl[KF];
+#pragma unroll
+  for (int i = 0; i < KF; ++i) {
+    rl[i] = 0.0;
+    if ((ow >> i) & 1u) {
+      const int32_t g = __ldg(fdofs + i * nf + c);
+      if (g >= 0) rl[i] = double(__ldg(xf + g));
+    }
+  }
+#pragma unroll
+  for (int j = 0; j < KC; ++j) {
+    const int32_t g = __ldg(cdofs + j * nc + pc);
+    if (g < 0) continue;
+    double acc = 0.0;
+#pragma unroll
+    for (int i = 0; i < KF; ++i) acc += __ldg(M + i * KC + j) * rl[i];
+    if (acc != 0.0) atomicAdd(xc + g, T(acc));
+  }
+}
+
 // DG p-transfer on one mesh: cell-local embedding P_{p-1} -> P_p, no sharing
 // (DG/cells_batched/application_phc.cc:3396-3475 builds the same two-level
 // transfer with MGTwoLevelTransfer on FE_SimplexDGP).  Layout [cell][K].
@@ -703,6 +771,16 @@ class MultigridImpl final : public Multigrid {
       SFEM_CUDA(cudaGetLastError());
       return;
     }
+#define SFEM_XFER(KF_, KC_)                                                                                \
+  if (F.Kf == KF_ && F.Kc == KC_) {                                                                        \
+    transfer_prolongate_add_k<T, KF_, KC_><<<grid, 128, 0, s>>>(                                           \
+        F.op->n_cells, F.parent.p, F.mat_id.p, F.owner.p, F.mats.p, F.op->device_dof_table(),               \
+        Cl.op->device_dof_table(), Cl.op->n_cells, static_cast<const T*>(src), static_cast<T*>(dst));       \
+    SFEM_CUDA(cudaGetLastError());                                                                        \
+    return;                                                                                               \
+  }
+    SFEM_XFER(20, 10) SFEM_XFER(10, 4) SFEM_XFER(4, 4) SFEM_XFER(10, 10) SFEM_XFER(20, 20)
+#undef SFEM_XFER
     transfer_prolongate_add<T><<<grid, 128, 0, s>>>(
         F.op->n_cells, F.Kf, F.Kc, F.parent.p, F.mat_id.p, F.owner.p, F.mats.p, F.op->device_dof_table(),
         Cl.op->device_dof_table(), Cl.op->n_cells, static_cast<const T*>(src), static_cast<T*>(dst));
@@ -726,6 +804,16 @@ class MultigridImpl final : public Multigrid {
       SFEM_CUDA(cudaGetLastError());
       return;
     }
+#define SFEM_XFER(KF_, KC_)                                                                                \
+  if (F.Kf == KF_ && F.Kc == KC_) {                                                                        \
+    transfer_restrict_add_k<T, KF_, KC_><<<grid, 128, 0, s>>>(                                             \
+        F.op->n_cells, F.parent.p, F.mat_id.p, F.owner.p, F.mats.p, F.op->device_dof_table(),               \
+        Cl.op->device_dof_table(), Cl.op->n_cells, static_cast<const T*>(src), static_cast<T*>(dst));       \
+    SFEM_CUDA(cudaGetLastError());                                                                        \
+    return;                                                                                               \
+  }
+    SFEM_XFER(20, 10) SFEM_XFER(10, 4) SFEM_XFER(4, 4) SFEM_XFER(10, 10) SFEM_XFER(20, 20)
+#undef SFEM_XFER
     transfer_restrict_add<T><<<grid, 128, 0, s>>>(
         F.op->n_cells, F.Kf, F.Kc, F.parent.p, F.mat_id.p, F.owner.p, F.mats.p, F.op->device_dof_table(),
         Cl.op->device_dof_table(), Cl.op->n_cells, static_cast<const T*>(src), static_cast<T*>(dst));
