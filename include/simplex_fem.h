@@ -82,7 +82,8 @@ typedef struct fem_op_params {
   int32_t penalty;         /* FEM_DG: enum fem_penalty */
   int32_t kernel_variant;  /* 0: tuned default; DG/Helmholtz: 1 thread per cell x128 cells per
                               CTA, 2 thread per cell x64, 3 warp roles x32, 4 thread per cell
-                              x64 with results in registers (scalar) and 8 CTAs per SM; CG: 1 thread per
+                              x64 with results in registers (scalar) and 8 CTAs per SM, 5 thread
+                              per cell x64 with 5 CTAs per SM; CG: 1 thread per
                               cell, 2 thread per Kuhn hex (6 tets, one atomic per distinct
                               DoF), 3 CTA per 4x4x4-hex Morton cube (stores for cube-interior
                               DoFs); each falls back to the next simpler form where the mesh
@@ -332,8 +333,8 @@ int fem_batch_set_kernel_variant(fem_batch* batch, int32_t variant);
  * Times every kernel variant (cells per CTA, thread or warp roles per cell;
  * fem_op_params.kernel_variant) of an operator or a batch with CUDA events
  * (median of `reps` launches after 2 warm-ups, on zero input), keeps the
- * fastest and returns it in *variant.  us[4] receives the median time per
- * variant 1..4 (0 = not a candidate; CG's approximate TF32 variant 4 is
+ * fastest and returns it in *variant.  us[5] receives the median time per
+ * variant 1..5 (0 = not a candidate; CG's approximate TF32 variant 4 is
  * never a candidate).  With use_cache != 0 a choice recorded for
  * the same (kind, degree, precision, components, log2 cells, GPU name) is
  * applied without timing (*cached = 1).  fem_autotune_cache sets a file that

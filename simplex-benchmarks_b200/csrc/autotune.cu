@@ -47,7 +47,7 @@ void load_file_locked() {
 
 std::vector<int> tune_candidates(const OpConfig& cfg) {
   if (cfg.kind == FEM_CG) return {1, 2, 3};
-  return {1, 2, 3, 4};
+  return {1, 2, 3, 4, 5};
 }
 
 std::string tune_key(const OpConfig& cfg, int64_t cells) {
@@ -107,7 +107,7 @@ void tune_set_cache_file(const std::string& path) {
 TuneResult autotune(Operator& op, int reps, bool use_cache) {
   TuneResult res;
   const std::vector<int> cand = tune_candidates(op.cfg);
-  res.us.assign(4, 0.0);
+  res.us.assign(5, 0.0);
   const std::string key = tune_key(op.cfg, op.n_cells);
   if (use_cache) {
     const int v = tune_lookup(key);

@@ -52,8 +52,8 @@ __device__ __forceinline__ void cg_local_apply(const T (&G)[6], const T (&u)[gen
 // sets to src (ones on the constrained diagonal).
 // dofs: [K][n_cells], -1 marks a constrained DoF (masked gather/scatter).
 // geo:  [6][n_cells] metric G.
-template <int P, typename T>
-__global__ void __launch_bounds__(128) cg_cell_kernel(int64_t n_cells, const int32_t* __restrict__ dofs,
+template <int P, typename T, int MINB = 1>
+__global__ void __launch_bounds__(128, MINB) cg_cell_kernel(int64_t n_cells, const int32_t* __restrict__ dofs,
                                                       const T* __restrict__ geo, const T* __restrict__ src,
                                                       T* __restrict__ dst, int64_t n_constrained,
                                                       const int32_t* __restrict__ constrained) {

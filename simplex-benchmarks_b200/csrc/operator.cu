@@ -426,7 +426,11 @@ class CGOperator final : public Operator {
     switch (cfg.degree) {
       case 1: cg_cell_kernel<1, T><<<grid, 128, 0, s>>>(n_cells, d_dofs.p, d_geo.p, x, d, d_constrained.n, d_constrained.p); break;
       case 2: cg_cell_kernel<2, T><<<grid, 128, 0, s>>>(n_cells, d_dofs.p, d_geo.p, x, d, d_constrained.n, d_constrained.p); break;
-      case 3: cg_cell_kernel<3, T><<<grid, 128, 0, s>>>(n_cells, d_dofs.p, d_geo.p, x, d, d_constrained.n, d_constrained.p); break;
+      case 3:
+        // P3 in FP64: registers capped for 4 CTAs per SM (measured faster on B200)
+        if (sizeof(T) == 8) cg_cell_kernel<3, T, 4><<<grid, 128, 0, s>>>(n_cells, d_dofs.p, d_geo.p, x, d, d_constrained.n, d_constrained.p);
+        else cg_cell_kernel<3, T><<<grid, 128, 0, s>>>(n_cells, d_dofs.p, d_geo.p, x, d, d_constrained.n, d_constrained.p);
+        break;
     }
     SFEM_CUDA(cudaGetLastError());
   }
@@ -678,13 +682,16 @@ class DGOperator final : public Operator {
       run_cell<P, NC, MASS, 64>(probs, n, s, what);
     } else if (variant == 3) {
       run_warp<P, NC, MASS>(probs, n, s, what);
+    } else if (variant == 5) {
+      // 64 cells per CTA, 5 CTAs per SM (up to 204 registers: no spills for P3)
+      run_cell<P, NC, MASS, 64, 5, false>(probs, n, s, what);
     } else if (variant == 4) {
       // 64 cells per CTA, results aliased onto the staged src rows (scalar
       // problems), registers capped for 8 CTAs per SM
       if (NC == 1) run_cell<P, NC, MASS, 64, 8, (NC == 1)>(probs, n, s, what);
       else run_cell<P, NC, MASS, 64, 8, false>(probs, n, s, what);
     } else {
-      throw Error(FEM_ERR_ARG, "DG: kernel variant must be 0..4");
+      throw Error(FEM_ERR_ARG, "DG: kernel variant must be 0..5");
     }
     SFEM_CUDA(cudaGetLastError());
   }
@@ -714,12 +721,12 @@ class DGBatchImpl final : public Batch {
   }
   int variant() const override { return cfg.kernel_variant; }
   void set_variant(int v) override {
-    SFEM_REQUIRE(v >= 0 && v <= 4, FEM_ERR_ARG, "batch: kernel variant must be 0..4");
+    SFEM_REQUIRE(v >= 0 && v <= 5, FEM_ERR_ARG, "batch: kernel variant must be 0..5");
     cfg.kernel_variant = v;
   }
   TuneResult tune(int reps, bool use_cache) override {
     TuneResult res;
-    res.us.assign(4, 0.0);
+    res.us.assign(5, 0.0);
     int64_t cells = 0;
     for (auto* o : ops) cells += o->n_cells;
     const std::string key = "batch" + std::to_string(ops.size()) + "," + tune_key(cfg, cells);

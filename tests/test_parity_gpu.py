@@ -238,7 +238,7 @@ def test_cg_tf32_tensor_core_variant(cuda, p):
         sf.Operator(mesh, p, "cg", "fp64").set_kernel_variant(4)
 
 
-@pytest.mark.parametrize("variant", [1, 2, 3, 4])
+@pytest.mark.parametrize("variant", [1, 2, 3, 4, 5])
 @pytest.mark.parametrize("kind", ["dg", "helmholtz"])
 @pytest.mark.parametrize("p", [1, 2, 3])
 def test_dg_kernel_variants(cuda, p, kind, variant):
