@@ -217,6 +217,114 @@ __global__ void __launch_bounds__(384) cg_cube_kernel(int64_t n_blocks, const in
   }
 }
 
+// Persistent, software-pipelined form of cg_cube_kernel: a CTA walks cubes
+// b0, b0 + G, b0 + 2G, ...  While it computes cube k, the gather of cube k+1
+// is already in flight as cp.async copies into the second of two shared
+// buffers, the DoF codes of cube k+2 and the tet metric of cube k+1 are being
+// loaded into registers, and the atomics of cube k-1 drain.  Buffer reuse is
+// ordered by the two block barriers of every iteration (a buffer is refilled
+// only after the barrier that follows its last read).
+// Shared memory: (2 NB + 384 KP) values.
+template <int P, typename T, int NB, int KP>
+__global__ void __launch_bounds__(384, P <= 2 ? 3 : (sizeof(T) == 4 ? 2 : 1)) cg_cube_pipe_kernel(int64_t n_blocks, const int16_t* __restrict__ tmap,
+                                                           const int32_t* __restrict__ bdof,
+                                                           const int16_t* __restrict__ rptr,
+                                                           const int16_t* __restrict__ rdof,
+                                                           const int16_t* __restrict__ cptr,
+                                                           const int16_t* __restrict__ cslot,
+                                                           const T* __restrict__ geo, const T* __restrict__ src,
+                                                           T* __restrict__ dst, int64_t n_constrained,
+                                                           const int32_t* __restrict__ constrained) {
+  using O = gen::Ops<P>;
+  constexpr int K = O::K;
+  constexpr int NJ = (NB + 383) / 384;  // cube DoFs gathered per thread
+  extern __shared__ __align__(16) unsigned char smem_cube[];
+  T* ubuf = reinterpret_cast<T*>(smem_cube);  // [2][NB]
+  T* yr = ubuf + 2 * NB;                      // [384][KP]
+  const int t = threadIdx.x;
+  const int64_t stride = gridDim.x;
+  const int64_t n_cells = n_blocks * 384;
+  for (int64_t i = blockIdx.x * int64_t(384) + t; i < n_constrained; i += stride * 384) {
+    const int32_t g = constrained[i];
+    dst[g] = src[g];
+  }
+  auto load_codes = [&](int64_t b, int32_t (&code)[NJ]) {
+#pragma unroll
+    for (int q = 0; q < NJ; ++q) {
+      const int j = t + 384 * q;
+      code[q] = (b < n_blocks && j < NB) ? __ldg(bdof + b * NB + j) : -1;
+    }
+  };
+  // cp.async of this thread's share of cube DoF values into buffer `buf`
+  auto issue_gather = [&](const int32_t (&code)[NJ], int buf, bool valid) {
+#pragma unroll
+    for (int q = 0; q < NJ; ++q) {
+      const int j = t + 384 * q;
+      if (!valid || j >= NB) continue;
+      T* d = ubuf + buf * NB + j;
+      if (code[q] < 0) {
+        *d = T(0);
+      } else {
+        const uint32_t sa = static_cast<uint32_t>(__cvta_generic_to_shared(d));
+        asm volatile("cp.async.ca.shared.global [%0], [%1], %2;" ::"r"(sa), "l"(src + (code[q] & 0x3FFFFFFF)),
+                     "n"(sizeof(T))
+                     : "memory");
+      }
+    }
+    asm volatile("cp.async.commit_group;" ::: "memory");
+  };
+  auto load_geo = [&](int64_t b, T (&G)[6]) {
+#pragma unroll
+    for (int k = 0; k < 6; ++k) G[k] = b < n_blocks ? __ldg(geo + k * n_cells + b * 384 + t) : T(0);
+  };
+
+  int64_t b = blockIdx.x;
+  int32_t code_cur[NJ], code_nxt[NJ];
+  T G[6], Gn[6];
+  load_codes(b, code_cur);
+  issue_gather(code_cur, 0, b < n_blocks);
+  load_codes(b + stride, code_nxt);
+  load_geo(b, G);
+  for (int k = 0; b < n_blocks; ++k, b += stride) {
+    const int buf = k & 1;
+    const bool more = b + stride < n_blocks;
+    // gather of the next cube, codes of the one after, metric of the next
+    issue_gather(code_nxt, buf ^ 1, more);
+#pragma unroll
+    for (int q = 0; q < NJ; ++q) code_cur[q] = code_nxt[q];
+    load_codes(b + 2 * stride, code_nxt);
+    load_geo(b + stride, Gn);
+    asm volatile("cp.async.wait_group 1;" ::: "memory");  // this cube's gather
+    __syncthreads();
+    {
+      const T* ub = ubuf + buf * NB;
+      T ut[K], yt[K];
+#pragma unroll
+      for (int i = 0; i < K; ++i) ut[i] = ub[__ldg(tmap + t * K + i)];
+      cg_local_apply<P>(G, ut, yt);
+#pragma unroll
+      for (int i = 0; i < K; ++i) yr[t * KP + i] = yt[i];
+    }
+    __syncthreads();
+    const int32_t* bd = bdof + b * NB;
+    const int r1 = __ldg(rptr + t + 1);
+    for (int r = __ldg(rptr + t); r < r1; ++r) {
+      const int j = __ldg(rdof + r);
+      const int32_t code = __ldg(bd + j);
+      if (code < 0) continue;
+      T sum = T(0);
+      const int e1 = __ldg(cptr + j + 1);
+      for (int e = __ldg(cptr + j); e < e1; ++e) sum += yr[__ldg(cslot + e)];
+      const int32_t g = code & 0x3FFFFFFF;
+      if (code & 0x40000000) dst[g] = sum;
+      else atomicAdd(dst + g, sum);
+    }
+#pragma unroll
+    for (int k6 = 0; k6 < 6; ++k6) G[k6] = Gn[k6];
+  }
+  asm volatile("cp.async.wait_group 0;" ::: "memory");
+}
+
 // Diagonal of the assembled operator: sum over cells of (A_K)_ii, constrained
 // rows get 1 (ones on the diagonal).  dst zero on entry.
 template <int P, typename T>

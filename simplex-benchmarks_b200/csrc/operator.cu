@@ -231,16 +231,23 @@ class CGOperator final : public Operator {
     SFEM_CUDA(cudaGetLastError());
   }
 
+  int cube_grid = 0;
   template <int P, int NB, int KP>
-  static size_t cube_smem() { return (size_t(NB) + 384 * size_t(KP)) * sizeof(T); }
+  static size_t cube_smem() { return (2 * size_t(NB) + 384 * size_t(KP)) * sizeof(T); }
   template <int P, int NB, int KP>
   void setup_cube() {
-    SFEM_CUDA(cudaFuncSetAttribute(cg_cube_kernel<P, T, NB, KP>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                   int(cube_smem<P, NB, KP>())));
+    auto kern = cg_cube_pipe_kernel<P, T, NB, KP>;
+    SFEM_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, int(cube_smem<P, NB, KP>())));
+    int dev = 0, sms = 0, occ = 0;
+    SFEM_CUDA(cudaGetDevice(&dev));
+    SFEM_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+    SFEM_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, kern, 384, cube_smem<P, NB, KP>()));
+    SFEM_REQUIRE(occ > 0, FEM_ERR_CUDA, "CG cube kernel does not fit on an SM");
+    cube_grid = int(std::min<int64_t>(n_blocks, int64_t(sms) * occ));
   }
   template <int P, int NB, int KP>
   void launch_cube(const T* x, T* d, cudaStream_t s) {
-    cg_cube_kernel<P, T, NB, KP><<<unsigned(n_blocks), 384, cube_smem<P, NB, KP>(), s>>>(
+    cg_cube_pipe_kernel<P, T, NB, KP><<<unsigned(cube_grid), 384, cube_smem<P, NB, KP>(), s>>>(
         n_blocks, d_tmap.p, d_bdof.p, d_rptr.p, d_rdof.p, d_cptr.p, d_cslot.p, d_geo.p, x, d, d_constrained.n,
         d_constrained.p);
   }
