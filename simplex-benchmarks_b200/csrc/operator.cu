@@ -456,6 +456,20 @@ class CGOperator final : public Operator {
   }
 
   const int32_t* device_dof_table() const override { return d_dofs.p; }
+  CubeTables cube_tables() const override {
+    CubeTables c;
+    if (!cube_NB) return c;
+    c.n_blocks = n_blocks;
+    c.NB = cube_NB;
+    c.KP = cube_kp(K);
+    c.tmap = d_tmap.p;
+    c.bdof = d_bdof.p;
+    c.rptr = d_rptr.p;
+    c.rdof = d_rdof.p;
+    c.cptr = d_cptr.p;
+    c.cslot = d_cslot.p;
+    return c;
+  }
 
   void work(double& flops, double& bytes) const override {
     const int p = cfg.degree, kq = kq_of(p);

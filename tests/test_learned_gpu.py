@@ -118,3 +118,25 @@ def test_fallback_to_chebyshev(cuda):
     bad.set_weights(np.random.default_rng(0).standard_normal(sf.mlp_n_params()).astype(np.float32) * 5)
     r = _solve(op, mg, b, bad, fallback=True)
     assert r["status"] == sf.FEM_OK and r["fallback_iteration"] >= 1, r
+
+
+def test_tensor_core_smoother_matches_cuda_cores(cuda):
+    """A learned V-cycle with the tensor-core smoother (BF16 activations)
+    agrees with the CUDA-core smoother (FP32 activations) to the BF16
+    tolerance (rel l2 <= 2e-2)."""
+    import torch
+    mesh = sf.Mesh(16)
+    op = sf.Operator(mesh, 3, "cg")
+    mlp = sf.MLP(seed=1)
+    mg = sf.Multigrid(op, precision="fp32", use_graph=False)
+    b = sf.rhs(op, sf.sine_modes_rhs())
+    out = []
+    for tc in (True, False):
+        mlp.set_tensor_cores(tc)
+        mg.set_learned_smoother(mlp, fallback=False)
+        x = op.initialize_dof_vector()
+        mg.vmult(x, b)
+        torch.cuda.synchronize()
+        out.append(x.cpu().numpy())
+    assert not mlp.timed_out()
+    assert np.linalg.norm(out[0] - out[1]) <= 2e-2 * np.linalg.norm(out[1])
