@@ -148,100 +148,47 @@ __global__ void __launch_bounds__(BS) cg_hex_kernel(int64_t n_hex, const int32_t
 
 // Cube-block form for Kuhn meshes whose hexes come in Morton order: 64
 // consecutive hexes (384 tets) form a 4 x 4 x 4 cube, and every cube has the
-// same local structure, so one set of small tables serves all blocks.  One
-// CTA per cube, one thread per tet:
-//   1. the cube's distinct DoFs (P1 125, P2 729) are gathered once into
-//      shared memory;
-//   2. each thread applies its tet's operator and writes the 20-or-fewer
-//      results to its shared-memory row;
+// same local structure, so one set of small tables serves all cubes.  One
+// thread per tet:
+//   1. the cube's distinct DoFs (P1 125, P2 729, P3 2197) are gathered once
+//      into shared memory;
+//   2. each thread applies its tet's operator and writes its K results to its
+//      shared-memory row;
 //   3. each distinct DoF sums its contributions (work split among the threads
-//      longest-first, so every thread sums ~K values) and is written back
-//      once: a plain store when only this cube touches it, else one atomic.
+//      longest-first) and is written back once: a plain store when only this
+//      cube touches it, else one atomic.
 // About 6 atomics per hex for P2 (27 with cg_hex_kernel, 60 with
-// cg_cell_kernel) and one gather per distinct DoF.
-// tmap  [384][K] cube-local DoF of tet t's local DoF i
+// cg_cell_kernel) and one gather per distinct DoF.  The tables are packed for
+// 16-byte loads (the kernel is bound by L1 / shared-memory transactions):
+// tmapv [384][KV] cube-local DoF of tet t's local DoF i (KV = K rounded up to 8)
 // bdof  [n_blocks][NB] global DoF | (interior << 30), -1 at constrained DoFs
-// rptr  [385], rdof: the cube DoFs thread t reduces (rdof[rptr[t] .. rptr[t+1]))
-// cptr  [NB+1], cslot: row slots (t * KP + i) holding the contributions of DoF j
-template <int P, typename T, int NB, int KP>
-__global__ void __launch_bounds__(384) cg_cube_kernel(int64_t n_blocks, const int16_t* __restrict__ tmap,
-                                                      const int32_t* __restrict__ bdof,
-                                                      const int16_t* __restrict__ rptr,
-                                                      const int16_t* __restrict__ rdof,
-                                                      const int16_t* __restrict__ cptr,
-                                                      const int16_t* __restrict__ cslot,
-                                                      const T* __restrict__ geo, const T* __restrict__ src,
-                                                      T* __restrict__ dst, int64_t n_constrained,
-                                                      const int32_t* __restrict__ constrained) {
-  using O = gen::Ops<P>;
-  constexpr int K = O::K;
-  extern __shared__ __align__(16) unsigned char smem_cube[];
-  T* ub = reinterpret_cast<T*>(smem_cube);  // [NB]
-  T* yr = ub + NB;                          // [384][KP]
-  const int t = threadIdx.x;
-  const int64_t b = blockIdx.x;
-  for (int64_t i = b * 384 + t; i < n_constrained; i += int64_t(gridDim.x) * 384) {
-    const int32_t g = constrained[i];
-    dst[g] = src[g];
-  }
-  const int32_t* bd = bdof + b * NB;
-  for (int j = t; j < NB; j += 384) {
-    const int32_t code = __ldg(bd + j);
-    ub[j] = code >= 0 ? __ldg(src + (code & 0x3FFFFFFF)) : T(0);
-  }
-  __syncthreads();
-  {
-    const int64_t n_cells = n_blocks * 384;
-    const int64_t c = b * 384 + t;
-    T G[6], ut[K], yt[K];
-#pragma unroll
-    for (int k = 0; k < 6; ++k) G[k] = __ldg(geo + k * n_cells + c);
-#pragma unroll
-    for (int i = 0; i < K; ++i) ut[i] = ub[__ldg(tmap + t * K + i)];
-    cg_local_apply<P>(G, ut, yt);
-#pragma unroll
-    for (int i = 0; i < K; ++i) yr[t * KP + i] = yt[i];
-  }
-  __syncthreads();
-  const int r1 = __ldg(rptr + t + 1);
-  for (int r = __ldg(rptr + t); r < r1; ++r) {
-    const int j = __ldg(rdof + r);
-    const int32_t code = __ldg(bd + j);
-    if (code < 0) continue;
-    T s = T(0);
-    const int e1 = __ldg(cptr + j + 1);
-    for (int e = __ldg(cptr + j); e < e1; ++e) s += yr[__ldg(cslot + e)];
-    const int32_t g = code & 0x3FFFFFFF;
-    if (code & 0x40000000) dst[g] = s;
-    else atomicAdd(dst + g, s);
-  }
-}
-
-// Persistent, software-pipelined form of cg_cube_kernel: a CTA walks cubes
-// b0, b0 + G, b0 + 2G, ...  While it computes cube k, the gather of cube k+1
+// rptr  [385], ritem: the DoFs thread t reduces, ritem = j | (g0 << 12) | (ng << 28)
+// cslot8: the contributing row slots (t * KP + i) of DoF j in ng groups of 8
+//       from group g0 on, padded with the zero slot 384 * KP
+// Persistent and software-pipelined: a CTA walks cubes b0, b0 + G, b0 + 2G,
+// ...  While it computes cube k, the gather of cube k+1
 // is already in flight as cp.async copies into the second of two shared
 // buffers, the DoF codes of cube k+2 and the tet metric of cube k+1 are being
 // loaded into registers, and the atomics of cube k-1 drain.  Buffer reuse is
 // ordered by the two block barriers of every iteration (a buffer is refilled
 // only after the barrier that follows its last read).
-// Shared memory: (2 NB + 384 KP) values.
+// Shared memory: (2 NB + 384 KP + 1) values.
 template <int P, typename T, int NB, int KP>
-__global__ void __launch_bounds__(384, P <= 2 ? 3 : (sizeof(T) == 4 ? 2 : 1)) cg_cube_pipe_kernel(int64_t n_blocks, const int16_t* __restrict__ tmap,
-                                                           const int32_t* __restrict__ bdof,
-                                                           const int16_t* __restrict__ rptr,
-                                                           const int16_t* __restrict__ rdof,
-                                                           const int16_t* __restrict__ cptr,
-                                                           const int16_t* __restrict__ cslot,
-                                                           const T* __restrict__ geo, const T* __restrict__ src,
-                                                           T* __restrict__ dst, int64_t n_constrained,
-                                                           const int32_t* __restrict__ constrained) {
+__global__ void __launch_bounds__(384, P <= 2 ? 3 : (sizeof(T) == 4 ? 2 : 1))
+    cg_cube_pipe_kernel(int64_t n_blocks, const int16_t* __restrict__ tmapv, const int32_t* __restrict__ bdof,
+                        const int16_t* __restrict__ rptr, const uint32_t* __restrict__ ritem,
+                        const int16_t* __restrict__ cslot8, const T* __restrict__ geo, const T* __restrict__ src,
+                        T* __restrict__ dst, int64_t n_constrained, const int32_t* __restrict__ constrained) {
   using O = gen::Ops<P>;
   constexpr int K = O::K;
+  constexpr int KV = (K + 7) / 8 * 8;
+  constexpr int ZERO = 384 * KP;  // the zero slot that pads the contribution groups
   constexpr int NJ = (NB + 383) / 384;  // cube DoFs gathered per thread
   extern __shared__ __align__(16) unsigned char smem_cube[];
   T* ubuf = reinterpret_cast<T*>(smem_cube);  // [2][NB]
-  T* yr = ubuf + 2 * NB;                      // [384][KP]
+  T* yr = ubuf + 2 * NB;                      // [384][KP] + the zero slot
   const int t = threadIdx.x;
+  if (t == 0) yr[ZERO] = T(0);
   const int64_t stride = gridDim.x;
   const int64_t n_cells = n_blocks * 384;
   for (int64_t i = blockIdx.x * int64_t(384) + t; i < n_constrained; i += stride * 384) {
@@ -298,9 +245,21 @@ __global__ void __launch_bounds__(384, P <= 2 ? 3 : (sizeof(T) == 4 ? 2 : 1)) cg
     __syncthreads();
     {
       const T* ub = ubuf + buf * NB;
+      const uint4* tm = reinterpret_cast<const uint4*>(tmapv + t * KV);
+      int ti[KV];
+#pragma unroll
+      for (int q = 0; q < KV / 8; ++q) {
+        const uint4 w = __ldg(tm + q);
+        const uint32_t wv[4] = {w.x, w.y, w.z, w.w};
+#pragma unroll
+        for (int h = 0; h < 4; ++h) {
+          ti[8 * q + 2 * h] = int(wv[h] & 0xFFFFu);
+          ti[8 * q + 2 * h + 1] = int(wv[h] >> 16);
+        }
+      }
       T ut[K], yt[K];
 #pragma unroll
-      for (int i = 0; i < K; ++i) ut[i] = ub[__ldg(tmap + t * K + i)];
+      for (int i = 0; i < K; ++i) ut[i] = ub[ti[i]];
       cg_local_apply<P>(G, ut, yt);
 #pragma unroll
       for (int i = 0; i < K; ++i) yr[t * KP + i] = yt[i];
@@ -309,12 +268,17 @@ __global__ void __launch_bounds__(384, P <= 2 ? 3 : (sizeof(T) == 4 ? 2 : 1)) cg
     const int32_t* bd = bdof + b * NB;
     const int r1 = __ldg(rptr + t + 1);
     for (int r = __ldg(rptr + t); r < r1; ++r) {
-      const int j = __ldg(rdof + r);
-      const int32_t code = __ldg(bd + j);
+      const uint32_t item = __ldg(ritem + r);
+      const int32_t code = __ldg(bd + (item & 0xFFFu));
       if (code < 0) continue;
+      const uint4* grp = reinterpret_cast<const uint4*>(cslot8) + ((item >> 12) & 0xFFFFu);
+      const int ng = int(item >> 28);
       T sum = T(0);
-      const int e1 = __ldg(cptr + j + 1);
-      for (int e = __ldg(cptr + j); e < e1; ++e) sum += yr[__ldg(cslot + e)];
+      for (int q = 0; q < ng; ++q) {
+        const uint4 w = __ldg(grp + q);
+        sum += yr[w.x & 0xFFFFu] + yr[w.x >> 16] + yr[w.y & 0xFFFFu] + yr[w.y >> 16] + yr[w.z & 0xFFFFu] +
+               yr[w.z >> 16] + yr[w.w & 0xFFFFu] + yr[w.w >> 16];
+      }
       const int32_t g = code & 0x3FFFFFFF;
       if (code & 0x40000000) dst[g] = sum;
       else atomicAdd(dst + g, sum);

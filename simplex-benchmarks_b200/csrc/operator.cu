@@ -122,7 +122,8 @@ class CGOperator final : public Operator {
   }
 
   // cube-block tables of cg_cube_kernel (blocks of 64 hexes = 384 tets)
-  DevBuf<int16_t> d_tmap, d_rptr, d_rdof, d_cptr, d_cslot;
+  DevBuf<int16_t> d_tmapv, d_rptr, d_cslot8;
+  DevBuf<uint32_t> d_ritem;
   DevBuf<int32_t> d_bdof;
   int64_t n_blocks = 0;
   int cube_NB = 0;
@@ -201,20 +202,35 @@ class CGOperator final : public Operator {
       per[th].push_back(int16_t(j));
       load[th] += int(contrib[j].size()) + 2;
     }
-    std::vector<int16_t> rptr(385, 0), rdof, cptr(NB + 1, 0), cslot;
+    // packed tables: tet maps padded to KV entries (16-byte rows); each DoF's
+    // contributions in groups of 8 slots padded with the zero slot 384 * KP;
+    // one 32-bit item per DoF: j | (first group << 12) | (groups << 28)
+    const int KV = (K + 7) / 8 * 8, ZERO = 384 * KP;
+    std::vector<int16_t> tmv(size_t(384) * KV, 0);
+    for (int t = 0; t < 384; ++t)
+      for (int i = 0; i < K; ++i) tmv[size_t(t) * KV + i] = tm0[t * K + i];
+    std::vector<int16_t> c8;
+    std::vector<uint32_t> g0(NB), ngr(NB);
+    for (int j = 0; j < NB; ++j) {
+      g0[j] = uint32_t(c8.size() / 8);
+      for (int16_t v : contrib[j]) c8.push_back(v);
+      while (c8.size() % 8) c8.push_back(int16_t(ZERO));
+      ngr[j] = uint32_t(c8.size() / 8) - g0[j];
+    }
+    SFEM_REQUIRE(c8.size() / 8 < 65536 && ZERO < 32768, FEM_ERR_INTERNAL, "cube tables exceed 16-bit indices");
+    std::vector<int16_t> rptr(385, 0);
+    std::vector<uint32_t> items;
     for (int th = 0; th < 384; ++th) {
       rptr[th + 1] = int16_t(rptr[th] + per[th].size());
-      rdof.insert(rdof.end(), per[th].begin(), per[th].end());
+      for (int16_t j : per[th]) {
+        SFEM_REQUIRE(ngr[j] < 16, FEM_ERR_INTERNAL, "cube tables: too many contributions to one DoF");
+        items.push_back(uint32_t(j) | (g0[j] << 12) | (ngr[j] << 28));
+      }
     }
-    for (int j = 0; j < NB; ++j) {
-      cptr[j + 1] = int16_t(cptr[j] + contrib[j].size());
-      cslot.insert(cslot.end(), contrib[j].begin(), contrib[j].end());
-    }
-    d_tmap.upload(tm0);
+    d_tmapv.upload(tmv);
     d_rptr.upload(rptr);
-    d_rdof.upload(rdof);
-    d_cptr.upload(cptr);
-    d_cslot.upload(cslot);
+    d_ritem.upload(items);
+    d_cslot8.upload(c8);
     d_bdof.upload(bd);
     n_blocks = nbk;
     cube_NB = NB;
@@ -233,7 +249,7 @@ class CGOperator final : public Operator {
 
   int cube_grid = 0;
   template <int P, int NB, int KP>
-  static size_t cube_smem() { return (2 * size_t(NB) + 384 * size_t(KP)) * sizeof(T); }
+  static size_t cube_smem() { return (2 * size_t(NB) + 384 * size_t(KP) + 1) * sizeof(T); }
   template <int P, int NB, int KP>
   void setup_cube() {
     auto kern = cg_cube_pipe_kernel<P, T, NB, KP>;
@@ -248,7 +264,7 @@ class CGOperator final : public Operator {
   template <int P, int NB, int KP>
   void launch_cube(const T* x, T* d, cudaStream_t s) {
     cg_cube_pipe_kernel<P, T, NB, KP><<<unsigned(cube_grid), 384, cube_smem<P, NB, KP>(), s>>>(
-        n_blocks, d_tmap.p, d_bdof.p, d_rptr.p, d_rdof.p, d_cptr.p, d_cslot.p, d_geo.p, x, d, d_constrained.n,
+        n_blocks, d_tmapv.p, d_bdof.p, d_rptr.p, d_ritem.p, d_cslot8.p, d_geo.p, x, d, d_constrained.n,
         d_constrained.p);
   }
 
@@ -456,20 +472,6 @@ class CGOperator final : public Operator {
   }
 
   const int32_t* device_dof_table() const override { return d_dofs.p; }
-  CubeTables cube_tables() const override {
-    CubeTables c;
-    if (!cube_NB) return c;
-    c.n_blocks = n_blocks;
-    c.NB = cube_NB;
-    c.KP = cube_kp(K);
-    c.tmap = d_tmap.p;
-    c.bdof = d_bdof.p;
-    c.rptr = d_rptr.p;
-    c.rdof = d_rdof.p;
-    c.cptr = d_cptr.p;
-    c.cslot = d_cslot.p;
-    return c;
-  }
 
   void work(double& flops, double& bytes) const override {
     const int p = cfg.degree, kq = kq_of(p);

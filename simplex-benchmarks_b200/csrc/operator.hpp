@@ -64,17 +64,6 @@ struct OpConfig {
   int kernel_variant = 0;  // 0: tuned default (see fem_op_params.kernel_variant)
 };
 
-// Cube-block tables of a CG operator on a Morton-ordered Kuhn mesh (4x4x4
-// hexes = 384 tets per cube, identical local structure in every cube); see
-// cg_cube_kernel.  n_blocks == 0: not available.
-struct CubeTables {
-  int64_t n_blocks = 0;
-  int NB = 0, KP = 0;
-  const int16_t* tmap = nullptr;
-  const int32_t* bdof = nullptr;
-  const int16_t *rptr = nullptr, *rdof = nullptr, *cptr = nullptr, *cslot = nullptr;
-};
-
 class Operator {
  public:
   virtual ~Operator() = default;
@@ -95,7 +84,6 @@ class Operator {
   virtual void diagonal(void* diag, cudaStream_t s) = 0;
   // CG: device table [K][n_cells] of global DoFs, -1 at constrained ones
   virtual const int32_t* device_dof_table() const { return nullptr; }
-  virtual CubeTables cube_tables() const { return CubeTables{}; }
   // Device scratch one vmult needs (DG: the published face traces; CG: none).
   virtual size_t scratch_bytes() const { return 0; }
   // vmult with the scratch supplied by the caller instead of the operator's own.
