@@ -724,6 +724,11 @@ template <typename T>
 class DGBatchImpl final : public Batch {
  public:
   std::vector<DGOperator<T>*> ops;
+  // an operator listed more than once (several right-hand sides on one mesh)
+  // gets a trace scratch of its own for every repeat: the two passes of one
+  // launch must not share it between problems
+  std::vector<DevBuf<T>> extra_q;
+  std::vector<int> q_of;  // -1: the operator's own scratch, else index into extra_q
   OpConfig cfg;
   explicit DGBatchImpl(const std::vector<Operator*>& o) {
     SFEM_REQUIRE(!o.empty() && int(o.size()) <= kMaxBatch, FEM_ERR_ARG, "batch: 1..40 operators");
@@ -734,12 +739,23 @@ class DGBatchImpl final : public Batch {
       SFEM_REQUIRE(d->cfg.degree == cfg.degree && d->cfg.kind == cfg.kind &&
                        d->cfg.n_components == cfg.n_components,
                    FEM_ERR_ARG, "batch: operators must share kind, degree and components");
+      int repeat = -1;
+      for (auto* prev : ops)
+        if (prev == d) repeat = 0;
+      if (repeat == 0) {
+        extra_q.emplace_back(d->scratch_bytes() / sizeof(T));
+        repeat = int(extra_q.size()) - 1;
+      }
+      q_of.push_back(repeat);
       ops.push_back(d);
     }
   }
   void vmult(void* const* dst, const void* const* src, cudaStream_t s) override {
     DGProblem<T> probs[kMaxBatch];
-    for (size_t i = 0; i < ops.size(); ++i) probs[i] = ops[i]->problem(src[i], dst[i]);
+    for (size_t i = 0; i < ops.size(); ++i) {
+      probs[i] = ops[i]->problem(src[i], dst[i]);
+      if (q_of[i] >= 0) probs[i].Q = extra_q[q_of[i]].p;
+    }
     DGOperator<T>::launch_dg(cfg, probs, int(ops.size()), s, 0);
   }
   int variant() const override { return cfg.kernel_variant; }

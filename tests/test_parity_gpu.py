@@ -250,3 +250,22 @@ def test_dg_kernel_variants(cuda, p, kind, variant):
     y = run_product(op, x)
     ref = orc.for_mesh(mesh, p, KIND[kind], n_components=op.n_components).vmult(x)
     assert rel_l2(y, ref) <= 1e-12
+
+
+@pytest.mark.parametrize("kind", ["dg", "helmholtz"])
+def test_batch_many_right_hand_sides_one_operator(cuda, kind):
+    """One operator listed several times in a batch applies it to several
+    vectors in one launch (each repeat gets its own trace scratch); every
+    result equals a separate vmult."""
+    import torch
+    mesh = sf.Mesh((5, 4, 3), jitter=0.1, seed=1)
+    op = sf.Operator(mesh, 2, kind, "fp64")
+    b = sf.Batch([op, op, op])
+    xs = [torch.tensor(seeded_src(op.m(), 20 + i), device="cuda") for i in range(3)]
+    ys = [op.initialize_dof_vector() for _ in range(3)]
+    b.vmult(ys, xs)
+    for x_, y_ in zip(xs, ys):
+        z = op.initialize_dof_vector()
+        op.vmult(z, x_)
+        torch.cuda.synchronize()
+        assert rel_l2(y_.cpu().numpy(), z.cpu().numpy()) <= 1e-13
