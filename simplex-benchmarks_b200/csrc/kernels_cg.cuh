@@ -162,9 +162,9 @@ __global__ void __launch_bounds__(BS) cg_hex_kernel(int64_t n_hex, const int32_t
 // 16-byte loads (the kernel is bound by L1 / shared-memory transactions):
 // tmapv [384][KV] cube-local DoF of tet t's local DoF i (KV = K rounded up to 8)
 // bdof  [n_blocks][NB] global DoF | (interior << 30), -1 at constrained DoFs
-// rptr  [385], ritem: the DoFs thread t reduces, ritem = j | (g0 << 12) | (ng << 28)
-// cslot8: the contributing row slots (t * KP + i) of DoF j in ng groups of 8
-//       from group g0 on, padded with the zero slot 384 * KP
+// rptr  [385], ritem: the DoFs thread t reduces, ritem = j | (g0 << 12) | (cnt << 27)
+// cslot8: the cnt contributing row slots (t * KP + i) of DoF j from group g0
+//       on (groups of 8, padded with the zero slot 384 * KP, not read)
 // Persistent and software-pipelined: a CTA walks cubes b0, b0 + G, b0 + 2G,
 // ...  While it computes cube k, the gather of cube k+1
 // is already in flight as cp.async copies into the second of two shared
@@ -271,13 +271,15 @@ __global__ void __launch_bounds__(384, P <= 2 ? 3 : (sizeof(T) == 4 ? 2 : 1))
       const uint32_t item = __ldg(ritem + r);
       const int32_t code = __ldg(bd + (item & 0xFFFu));
       if (code < 0) continue;
-      const uint4* grp = reinterpret_cast<const uint4*>(cslot8) + ((item >> 12) & 0xFFFFu);
-      const int ng = int(item >> 28);
+      const uint4* grp = reinterpret_cast<const uint4*>(cslot8) + ((item >> 12) & 0x7FFFu);
+      const int cnt = int(item >> 27);
       T sum = T(0);
-      for (int q = 0; q < ng; ++q) {
+      for (int q = 0; 8 * q < cnt; ++q) {
         const uint4 w = __ldg(grp + q);
-        sum += yr[w.x & 0xFFFFu] + yr[w.x >> 16] + yr[w.y & 0xFFFFu] + yr[w.y >> 16] + yr[w.z & 0xFFFFu] +
-               yr[w.z >> 16] + yr[w.w & 0xFFFFu] + yr[w.w >> 16];
+        const uint32_t wv[4] = {w.x, w.y, w.z, w.w};
+#pragma unroll
+        for (int h = 0; h < 8; ++h)  // padding slots are not read
+          if (8 * q + h < cnt) sum += yr[(h & 1) ? (wv[h >> 1] >> 16) : (wv[h >> 1] & 0xFFFFu)];
       }
       const int32_t g = code & 0x3FFFFFFF;
       if (code & 0x40000000) dst[g] = sum;

@@ -204,7 +204,7 @@ class CGOperator final : public Operator {
     }
     // packed tables: tet maps padded to KV entries (16-byte rows); each DoF's
     // contributions in groups of 8 slots padded with the zero slot 384 * KP;
-    // one 32-bit item per DoF: j | (first group << 12) | (groups << 28)
+    // one 32-bit item per DoF: j | (first group << 12) | (contributions << 27)
     const int KV = (K + 7) / 8 * 8, ZERO = 384 * KP;
     std::vector<int16_t> tmv(size_t(384) * KV, 0);
     for (int t = 0; t < 384; ++t)
@@ -217,14 +217,14 @@ class CGOperator final : public Operator {
       while (c8.size() % 8) c8.push_back(int16_t(ZERO));
       ngr[j] = uint32_t(c8.size() / 8) - g0[j];
     }
-    SFEM_REQUIRE(c8.size() / 8 < 65536 && ZERO < 32768, FEM_ERR_INTERNAL, "cube tables exceed 16-bit indices");
+    SFEM_REQUIRE(c8.size() / 8 < 32768 && ZERO < 32768, FEM_ERR_INTERNAL, "cube tables exceed their index bits");
     std::vector<int16_t> rptr(385, 0);
     std::vector<uint32_t> items;
     for (int th = 0; th < 384; ++th) {
       rptr[th + 1] = int16_t(rptr[th] + per[th].size());
       for (int16_t j : per[th]) {
-        SFEM_REQUIRE(ngr[j] < 16, FEM_ERR_INTERNAL, "cube tables: too many contributions to one DoF");
-        items.push_back(uint32_t(j) | (g0[j] << 12) | (ngr[j] << 28));
+        SFEM_REQUIRE(contrib[j].size() < 32, FEM_ERR_INTERNAL, "cube tables: too many contributions to one DoF");
+        items.push_back(uint32_t(j) | (g0[j] << 12) | (uint32_t(contrib[j].size()) << 27));
       }
     }
     d_tmapv.upload(tmv);
