@@ -154,17 +154,21 @@ __global__ void __launch_bounds__(BS) cg_hex_kernel(int64_t n_hex, const int32_t
 //      into shared memory;
 //   2. each thread applies its tet's operator and writes its K results to its
 //      shared-memory row;
-//   3. each distinct DoF sums its contributions (work split among the threads
-//      longest-first) and is written back once: a plain store when only this
-//      cube touches it, else one atomic.
+//   3. each distinct DoF sums its contributions and is written back once: a
+//      plain store when only this cube touches it, else one atomic.
 // About 6 atomics per hex for P2 (27 with cg_hex_kernel, 60 with
-// cg_cell_kernel) and one gather per distinct DoF.  The tables are packed for
-// 16-byte loads (the kernel is bound by L1 / shared-memory transactions):
-// tmapv [384][KV] cube-local DoF of tet t's local DoF i (KV = K rounded up to 8)
-// bdof  [n_blocks][NB] global DoF | (interior << 30), -1 at constrained DoFs
-// rptr  [385], ritem: the DoFs thread t reduces, ritem = j | (g0 << 12) | (cnt << 27)
-// cslot8: the cnt contributing row slots (t * KP + i) of DoF j from group g0
-//       on (groups of 8, padded with the zero slot 384 * KP, not read)
+// cg_cell_kernel) and one gather per distinct DoF.  The kernel is bound by L1 /
+// shared-memory transactions, so the tables are packed for 16-byte loads and
+// laid out [row][thread] (a warp reads one contiguous 512-byte row):
+// cube DoFs are numbered by reduce slot n = 384 r + t (thread t gathers and
+// reduces slot n in round r; a warp-round holds 32 DoFs with the same number
+// of contribution groups, so its lanes loop the same number of times);
+// tmapv  [KV/8][384] x 8: slot of tet t's local DoF i (KV = K rounded up to 8)
+// bdof   [n_blocks][NB] global DoF | (interior << 30), -1 at constrained DoFs
+// ritem  [NB]: contributions | (first cslot8 row entry << 8)
+// cslot8 per warp-round [groups][32] x 8: the contributing row slots
+//        (t * KP + i) of a slot, 8 per group, padded with the zero slot
+//        384 * KP (not read)
 // Persistent and software-pipelined: a CTA walks cubes b0, b0 + G, b0 + 2G,
 // ...  While it computes cube k, the gather of cube k+1
 // is already in flight as cp.async copies into the second of two shared
@@ -176,8 +180,7 @@ __global__ void __launch_bounds__(BS) cg_hex_kernel(int64_t n_hex, const int32_t
 template <int P, typename T, int NB, int KP>
 __global__ void __launch_bounds__(384, P <= 2 ? 3 : (sizeof(T) == 4 ? 2 : 1))
     cg_cube_pipe_kernel(int64_t n_blocks, const int16_t* __restrict__ tmapv, const int32_t* __restrict__ bdof,
-                        const int16_t* __restrict__ rptr, const uint32_t* __restrict__ ritem,
-                        const int16_t* __restrict__ cslot8, const T* __restrict__ geo, const T* __restrict__ src,
+                        const uint32_t* __restrict__ ritem, const int16_t* __restrict__ cslot8, const T* __restrict__ geo, const T* __restrict__ src,
                         T* __restrict__ dst, int64_t n_constrained, const int32_t* __restrict__ constrained) {
   using O = gen::Ops<P>;
   constexpr int K = O::K;
@@ -245,11 +248,11 @@ __global__ void __launch_bounds__(384, P <= 2 ? 3 : (sizeof(T) == 4 ? 2 : 1))
     __syncthreads();
     {
       const T* ub = ubuf + buf * NB;
-      const uint4* tm = reinterpret_cast<const uint4*>(tmapv + t * KV);
+      const uint4* tm = reinterpret_cast<const uint4*>(tmapv) + t;
       int ti[KV];
 #pragma unroll
       for (int q = 0; q < KV / 8; ++q) {
-        const uint4 w = __ldg(tm + q);
+        const uint4 w = __ldg(tm + 384 * q);
         const uint32_t wv[4] = {w.x, w.y, w.z, w.w};
 #pragma unroll
         for (int h = 0; h < 4; ++h) {
@@ -266,16 +269,18 @@ __global__ void __launch_bounds__(384, P <= 2 ? 3 : (sizeof(T) == 4 ? 2 : 1))
     }
     __syncthreads();
     const int32_t* bd = bdof + b * NB;
-    const int r1 = __ldg(rptr + t + 1);
-    for (int r = __ldg(rptr + t); r < r1; ++r) {
-      const uint32_t item = __ldg(ritem + r);
-      const int32_t code = __ldg(bd + (item & 0xFFFu));
+#pragma unroll 1
+    for (int r = 0; r < NJ; ++r) {
+      const int n = 384 * r + t;
+      if (n >= NB) break;
+      const int32_t code = __ldg(bd + n);
       if (code < 0) continue;
-      const uint4* grp = reinterpret_cast<const uint4*>(cslot8) + ((item >> 12) & 0x7FFFu);
-      const int cnt = int(item >> 27);
+      const uint32_t item = __ldg(ritem + n);
+      const uint4* grp = reinterpret_cast<const uint4*>(cslot8) + (item >> 8);
+      const int cnt = int(item & 0xFFu);
       T sum = T(0);
       for (int q = 0; 8 * q < cnt; ++q) {
-        const uint4 w = __ldg(grp + q);
+        const uint4 w = __ldg(grp + 32 * q);
         const uint32_t wv[4] = {w.x, w.y, w.z, w.w};
 #pragma unroll
         for (int h = 0; h < 8; ++h)  // padding slots are not read

@@ -122,7 +122,7 @@ class CGOperator final : public Operator {
   }
 
   // cube-block tables of cg_cube_kernel (blocks of 64 hexes = 384 tets)
-  DevBuf<int16_t> d_tmapv, d_rptr, d_cslot8;
+  DevBuf<int16_t> d_tmapv, d_cslot8;
   DevBuf<uint32_t> d_ritem;
   DevBuf<int32_t> d_bdof;
   int64_t n_blocks = 0;
@@ -165,6 +165,51 @@ class CGOperator final : public Operator {
     std::vector<std::vector<int16_t>> contrib(NB);
     for (int t = 0; t < 384; ++t)
       for (int i = 0; i < K; ++i) contrib[tm0[t * K + i]].push_back(int16_t(t * KP + i));
+    // reduce slots: slot n = 384 r + 32 w + l is gathered and reduced by lane
+    // l of warp w in round r.  DoFs sorted by contribution groups of 8
+    // (most first; first-occurrence order inside a class, which keeps the
+    // global addresses of a warp's gathers and stores close) form chunks of
+    // 32 that fill one warp-round each, so the lanes of a warp loop over the
+    // same number of groups; the chunks are dealt longest-first to the
+    // least-loaded warp, which balances the warps up to the block barrier.
+    std::vector<int> jorder(NB), slot_of(NB), dof_at(NB);
+    for (int j = 0; j < NB; ++j) jorder[j] = j;
+    std::stable_sort(jorder.begin(), jorder.end(), [&](int a, int b2) {
+      return (contrib[a].size() + 7) / 8 > (contrib[b2].size() + 7) / 8;
+    });
+    {
+      constexpr int NW = 12;
+      const int NJr = (NB + 383) / 384, nch = (NB + 31) / 32;
+      std::vector<int> cap(NW, 0), used(NW, 0), load(NW, 0), base(nch, -1);
+      for (int r = 0; r < NJr; ++r)
+        for (int w = 0; w < NW; ++w) {
+          const int len = std::max(0, std::min(32, NB - (384 * r + 32 * w)));
+          if (len == 32) ++cap[w];
+          else if (len > 0) base[nch - 1] = 384 * r + 32 * w;  // the one partial chunk
+        }
+      auto cost = [&](int c) {
+        int mx = 0;
+        for (int e = 32 * c; e < std::min(NB, 32 * c + 32); ++e) mx = std::max(mx, int(contrib[jorder[e]].size()));
+        return mx + 2 * ((mx + 7) / 8) + 4;
+      };
+      std::vector<int> corder;
+      for (int c = 0; c < nch; ++c)
+        if (base[c] < 0) corder.push_back(c);
+      std::stable_sort(corder.begin(), corder.end(), [&](int a, int b2) { return cost(a) > cost(b2); });
+      for (int c : corder) {
+        int w = -1;
+        for (int v = 0; v < NW; ++v)
+          if (used[v] < cap[v] && (w < 0 || load[v] < load[w])) w = v;
+        SFEM_REQUIRE(w >= 0, FEM_ERR_INTERNAL, "cube tables: no warp-round left for a chunk");
+        base[c] = 384 * used[w] + 32 * w;
+        ++used[w];
+        load[w] += cost(c);
+      }
+      for (int e = 0; e < NB; ++e) {
+        slot_of[jorder[e]] = base[e / 32] + e % 32;
+        dof_at[base[e / 32] + e % 32] = jorder[e];
+      }
+    }
     std::vector<int32_t> count(m, 0);
     for (size_t i = 0; i < dofs.cell_dofs.size(); ++i) ++count[dofs.cell_dofs[i]];
     std::vector<int32_t> bd(size_t(NB) * nbk);
@@ -182,53 +227,46 @@ class CGOperator final : public Operator {
           ok = false;
           continue;
         }
-        for (int j = 0; j < NB; ++j) {
+        for (int n = 0; n < NB; ++n) {
+          const int j = dof_at[n];
           const int32_t g = ord[j];
           const bool interior = count[g] == int(contrib[j].size());
-          bd[size_t(b) * NB + j] = dofs.constrained[g] ? -1 : (g | (interior ? 0x40000000 : 0));
+          bd[size_t(b) * NB + n] = dofs.constrained[g] ? -1 : (g | (interior ? 0x40000000 : 0));
         }
       }
     }
     if (!ok || m >= (int64_t(1) << 30)) return;
-    // reduce work: DoFs dealt longest-first to the least-loaded thread
-    std::vector<int> jorder(NB);
-    for (int j = 0; j < NB; ++j) jorder[j] = j;
-    std::stable_sort(jorder.begin(), jorder.end(),
-                     [&](int a, int b2) { return contrib[a].size() > contrib[b2].size(); });
-    std::vector<std::vector<int16_t>> per(384);
-    std::vector<int> load(384, 0);
-    for (int j : jorder) {
-      const int th = int(std::min_element(load.begin(), load.end()) - load.begin());
-      per[th].push_back(int16_t(j));
-      load[th] += int(contrib[j].size()) + 2;
-    }
-    // packed tables: tet maps padded to KV entries (16-byte rows); each DoF's
-    // contributions in groups of 8 slots padded with the zero slot 384 * KP;
-    // one 32-bit item per DoF: j | (first group << 12) | (contributions << 27)
+    // packed tables, laid out so that a warp reads 16 consecutive bytes per
+    // lane:
+    //   tmapv  [KV/8][384] x 8 int16: slot of tet t's local DoF i (KV = K
+    //          rounded up to 8, padding entries 0);
+    //   cslot8 per warp-round, [groups][32 lanes] x 8 int16: contributing row
+    //          slots (t' * KP + i) of each slot, padded with the zero slot
+    //          384 * KP (not read);
+    //   ritem  [NB]: contributions | (first cslot8 entry << 8).
     const int KV = (K + 7) / 8 * 8, ZERO = 384 * KP;
     std::vector<int16_t> tmv(size_t(384) * KV, 0);
     for (int t = 0; t < 384; ++t)
-      for (int i = 0; i < K; ++i) tmv[size_t(t) * KV + i] = tm0[t * K + i];
+      for (int i = 0; i < K; ++i) tmv[(size_t(i / 8) * 384 + t) * 8 + i % 8] = int16_t(slot_of[tm0[t * K + i]]);
     std::vector<int16_t> c8;
-    std::vector<uint32_t> g0(NB), ngr(NB);
-    for (int j = 0; j < NB; ++j) {
-      g0[j] = uint32_t(c8.size() / 8);
-      for (int16_t v : contrib[j]) c8.push_back(v);
-      while (c8.size() % 8) c8.push_back(int16_t(ZERO));
-      ngr[j] = uint32_t(c8.size() / 8) - g0[j];
-    }
-    SFEM_REQUIRE(c8.size() / 8 < 32768 && ZERO < 32768, FEM_ERR_INTERNAL, "cube tables exceed their index bits");
-    std::vector<int16_t> rptr(385, 0);
-    std::vector<uint32_t> items;
-    for (int th = 0; th < 384; ++th) {
-      rptr[th + 1] = int16_t(rptr[th] + per[th].size());
-      for (int16_t j : per[th]) {
-        SFEM_REQUIRE(contrib[j].size() < 32, FEM_ERR_INTERNAL, "cube tables: too many contributions to one DoF");
-        items.push_back(uint32_t(j) | (g0[j] << 12) | (uint32_t(contrib[j].size()) << 27));
+    std::vector<uint32_t> items(NB);
+    for (int n0 = 0; n0 < NB; n0 += 32) {
+      const int len = std::min(32, NB - n0);
+      size_t mx = 0;
+      for (int l = 0; l < len; ++l) mx = std::max(mx, contrib[dof_at[n0 + l]].size());
+      const size_t e0 = c8.size() / 8;
+      c8.resize(c8.size() + (mx + 7) / 8 * 32 * 8, int16_t(ZERO));
+      for (int l = 0; l < len; ++l) {
+        const std::vector<int16_t>& cl = contrib[dof_at[n0 + l]];
+        SFEM_REQUIRE(!cl.empty() && cl.size() < 256, FEM_ERR_INTERNAL,
+                     "cube tables: contribution count out of range");
+        for (size_t e = 0; e < cl.size(); ++e) c8[((e0 + e / 8 * 32) + l) * 8 + e % 8] = cl[e];
+        items[n0 + l] = uint32_t(cl.size()) | (uint32_t(e0 + l) << 8);
       }
     }
+    SFEM_REQUIRE(ZERO < 32768 && c8.size() / 8 < (size_t(1) << 24), FEM_ERR_INTERNAL,
+                 "cube tables exceed their index bits");
     d_tmapv.upload(tmv);
-    d_rptr.upload(rptr);
     d_ritem.upload(items);
     d_cslot8.upload(c8);
     d_bdof.upload(bd);
@@ -264,7 +302,7 @@ class CGOperator final : public Operator {
   template <int P, int NB, int KP>
   void launch_cube(const T* x, T* d, cudaStream_t s) {
     cg_cube_pipe_kernel<P, T, NB, KP><<<unsigned(cube_grid), 384, cube_smem<P, NB, KP>(), s>>>(
-        n_blocks, d_tmapv.p, d_bdof.p, d_rptr.p, d_ritem.p, d_cslot8.p, d_geo.p, x, d, d_constrained.n,
+        n_blocks, d_tmapv.p, d_bdof.p, d_ritem.p, d_cslot8.p, d_geo.p, x, d, d_constrained.n,
         d_constrained.p);
   }
 
