@@ -90,7 +90,11 @@ typedef struct fem_op_params {
                               lacks the pattern; default P1 2, P2 3, P3 3 (FP32) / 1 (FP64);
                               4: FP32 CG on the TF32 tensor cores (tcgen05 kind::tf32, cell
                               operator as one [128 cells x K] x [K x 6K] product; ~1e-3
-                              relative accuracy, for multigrid levels) */
+                              relative accuracy, for multigrid levels); CG 5, 6, 7: the cube
+                              kernel (3) with its DoF reduction read in contribution order
+                              (5), bank-scheduled with the same steps per warp (6) or
+                              bank-scheduled with per-lane steps (7); 3 takes the fastest
+                              measured on B200 (6 for FP64 P2, else 5) */
   int32_t reserved[5];
 } fem_op_params;
 
@@ -333,9 +337,9 @@ int fem_batch_set_kernel_variant(fem_batch* batch, int32_t variant);
  * Times every kernel variant (cells per CTA, thread or warp roles per cell;
  * fem_op_params.kernel_variant) of an operator or a batch with CUDA events
  * (median of `reps` launches after 2 warm-ups, on zero input), keeps the
- * fastest and returns it in *variant.  us[5] receives the median time per
- * variant 1..5 (0 = not a candidate; CG's approximate TF32 variant 4 is
- * never a candidate).  With use_cache != 0 a choice recorded for
+ * fastest and returns it in *variant.  us[8] receives the median time per
+ * variant 1..8 (0 = not a candidate; CG's approximate TF32 variant 4 is
+ * never a candidate, and CG's cube variant 3 is timed as 5, 6 and 7).  With use_cache != 0 a choice recorded for
  * the same (kind, degree, precision, components, log2 cells, GPU name) is
  * applied without timing (*cached = 1).  fem_autotune_cache sets a file that
  * keeps the choices across processes (JSON lines; NULL = memory only).

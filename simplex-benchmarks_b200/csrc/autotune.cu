@@ -46,7 +46,7 @@ void load_file_locked() {
 }  // namespace
 
 std::vector<int> tune_candidates(const OpConfig& cfg) {
-  if (cfg.kind == FEM_CG) return {1, 2, 3};
+  if (cfg.kind == FEM_CG) return {1, 2, 5, 6, 7};
   return {1, 2, 3, 4, 5};
 }
 
@@ -107,7 +107,7 @@ void tune_set_cache_file(const std::string& path) {
 TuneResult autotune(Operator& op, int reps, bool use_cache) {
   TuneResult res;
   const std::vector<int> cand = tune_candidates(op.cfg);
-  res.us.assign(5, 0.0);
+  res.us.assign(8, 0.0);
   const std::string key = tune_key(op.cfg, op.n_cells);
   if (use_cache) {
     const int v = tune_lookup(key);

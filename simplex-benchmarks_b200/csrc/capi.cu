@@ -124,7 +124,10 @@ int fem_op_create(fem_mesh* mesh, int32_t degree, int32_t kind, int32_t precisio
       }
       cfg.penalty = params->penalty;
       cfg.kernel_variant = params->kernel_variant;
-      SFEM_REQUIRE(cfg.kernel_variant >= 0 && cfg.kernel_variant <= 5, FEM_ERR_ARG, "kernel_variant must be 0..5");
+      SFEM_REQUIRE(cfg.kernel_variant >= 0 && cfg.kernel_variant <= (kind == FEM_CG ? 7 : 5), FEM_ERR_ARG,
+                   "kernel_variant must be 0..7 (CG) or 0..5 (DG, Helmholtz)");
+      SFEM_REQUIRE(cfg.kernel_variant != 4 || kind != FEM_CG || precision == FEM_FP32, FEM_ERR_ARG,
+                   "CG kernel_variant 4 (TF32 tensor cores) is for FP32 operators");
       SFEM_REQUIRE(cfg.penalty == FEM_PENALTY_REFERENCE || cfg.penalty == FEM_PENALTY_SQUARE, FEM_ERR_ARG,
                    "penalty must be FEM_PENALTY_REFERENCE or FEM_PENALTY_SQUARE");
     }
@@ -234,8 +237,8 @@ int fem_op_compute_diagonal(fem_op* op, void* diag, void* stream) {
 int fem_op_set_kernel_variant(fem_op* op, int32_t variant) {
   return guarded([&] {
     REQUIRE_PTR(op);
-    SFEM_REQUIRE(variant >= 0 && variant <= 5, FEM_ERR_ARG, "kernel_variant must be 0..5");
-    SFEM_REQUIRE(variant != 5 || op->op->cfg.kind != FEM_CG, FEM_ERR_ARG, "CG kernel variants are 0..4");
+    SFEM_REQUIRE(variant >= 0 && variant <= (op->op->cfg.kind == FEM_CG ? 7 : 5), FEM_ERR_ARG,
+                 "kernel_variant must be 0..7 (CG) or 0..5 (DG, Helmholtz)");
     SFEM_REQUIRE(variant != 4 || op->op->cfg.kind != FEM_CG || op->op->cfg.precision == FEM_FP32, FEM_ERR_ARG,
                  "CG kernel_variant 4 (TF32 tensor cores) is for FP32 operators");
     op->op->cfg.kernel_variant = variant;
@@ -287,7 +290,7 @@ int fem_op_autotune(fem_op* op, int32_t reps, int32_t use_cache, int32_t* varian
     if (variant) *variant = r.variant;
     if (cached) *cached = r.cached ? 1 : 0;
     if (us)
-      for (int i = 0; i < 5; ++i) us[i] = i < int(r.us.size()) ? r.us[i] : 0.0;
+      for (int i = 0; i < 8; ++i) us[i] = i < int(r.us.size()) ? r.us[i] : 0.0;
   });
 }
 
@@ -299,7 +302,7 @@ int fem_batch_autotune(fem_batch* batch, int32_t reps, int32_t use_cache, int32_
     if (variant) *variant = r.variant;
     if (cached) *cached = r.cached ? 1 : 0;
     if (us)
-      for (int i = 0; i < 5; ++i) us[i] = i < int(r.us.size()) ? r.us[i] : 0.0;
+      for (int i = 0; i < 8; ++i) us[i] = i < int(r.us.size()) ? r.us[i] : 0.0;
   });
 }
 

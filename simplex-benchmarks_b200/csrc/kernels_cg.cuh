@@ -161,14 +161,14 @@ __global__ void __launch_bounds__(BS) cg_hex_kernel(int64_t n_hex, const int32_t
 // shared-memory transactions, so the tables are packed for 16-byte loads and
 // laid out [row][thread] (a warp reads one contiguous 512-byte row):
 // cube DoFs are numbered by reduce slot n = 384 r + t (thread t gathers and
-// reduces slot n in round r; a warp-round holds 32 DoFs with the same number
-// of contribution groups, so its lanes loop the same number of times);
+// reduces slot n in round r; a warp-round holds 32 DoFs with similar
+// contribution counts);
 // tmapv  [KV/8][384] x 8: slot of tet t's local DoF i (KV = K rounded up to 8)
 // bdof   [n_blocks][NB] global DoF | (interior << 30), -1 at constrained DoFs
-// ritem  [NB]: contributions | (first cslot8 row entry << 8)
-// cslot8 per warp-round [groups][32] x 8: the contributing row slots
-//        (t * KP + i) of a slot, 8 per group, padded with the zero slot
-//        384 * KP (not read)
+// ritem  [NB]: steps of the warp-round | (first cslot8 entry << 8)
+// cslot8 per warp-round [groups][32] x 8: the row slot (t * KP + i) each
+//        lane reads at each step, or a zero slot 384 KP + z; the steps are
+//        scheduled so that no two lanes of a step read the same bank
 // Persistent and software-pipelined: a CTA walks cubes b0, b0 + G, b0 + 2G,
 // ...  While it computes cube k, the gather of cube k+1
 // is already in flight as cp.async copies into the second of two shared
@@ -176,22 +176,22 @@ __global__ void __launch_bounds__(BS) cg_hex_kernel(int64_t n_hex, const int32_t
 // loaded into registers, and the atomics of cube k-1 drain.  Buffer reuse is
 // ordered by the two block barriers of every iteration (a buffer is refilled
 // only after the barrier that follows its last read).
-// Shared memory: (2 NB + 384 KP + 1) values.
+// Shared memory: (2 NB + 384 KP + NZ) values, NZ = 16 zero slots for 8-byte
+// values (bank pairs), 32 for 4-byte values.
 template <int P, typename T, int NB, int KP>
 __global__ void __launch_bounds__(384, P <= 2 ? 3 : (sizeof(T) == 4 ? 2 : 1))
     cg_cube_pipe_kernel(int64_t n_blocks, const int16_t* __restrict__ tmapv, const int32_t* __restrict__ bdof,
-                        const uint32_t* __restrict__ ritem, const int16_t* __restrict__ cslot8, const T* __restrict__ geo, const T* __restrict__ src,
-                        T* __restrict__ dst, int64_t n_constrained, const int32_t* __restrict__ constrained) {
+                        const uint32_t* __restrict__ ritem, const int16_t* __restrict__ cslot8,
+                        const T* __restrict__ geo, const T* __restrict__ src, T* __restrict__ dst, int64_t n_constrained, const int32_t* __restrict__ constrained) {
   using O = gen::Ops<P>;
   constexpr int K = O::K;
   constexpr int KV = (K + 7) / 8 * 8;
-  constexpr int ZERO = 384 * KP;  // the zero slot that pads the contribution groups
   constexpr int NJ = (NB + 383) / 384;  // cube DoFs gathered per thread
   extern __shared__ __align__(16) unsigned char smem_cube[];
   T* ubuf = reinterpret_cast<T*>(smem_cube);  // [2][NB]
-  T* yr = ubuf + 2 * NB;                      // [384][KP] + the zero slot
+  T* yr = ubuf + 2 * NB;                      // [384][KP], then the zero slots
   const int t = threadIdx.x;
-  if (t == 0) yr[ZERO] = T(0);
+  if (t < (sizeof(T) == 8 ? 16 : 32)) yr[384 * KP + t] = T(0);
   const int64_t stride = gridDim.x;
   const int64_t n_cells = n_blocks * 384;
   for (int64_t i = blockIdx.x * int64_t(384) + t; i < n_constrained; i += stride * 384) {
@@ -277,14 +277,14 @@ __global__ void __launch_bounds__(384, P <= 2 ? 3 : (sizeof(T) == 4 ? 2 : 1))
       if (code < 0) continue;
       const uint32_t item = __ldg(ritem + n);
       const uint4* grp = reinterpret_cast<const uint4*>(cslot8) + (item >> 8);
-      const int cnt = int(item & 0xFFu);
+      const int steps = int(item & 0xFFu);  // the same for every lane of the warp
       T sum = T(0);
-      for (int q = 0; 8 * q < cnt; ++q) {
+      for (int q = 0; 8 * q < steps; ++q) {
         const uint4 w = __ldg(grp + 32 * q);
         const uint32_t wv[4] = {w.x, w.y, w.z, w.w};
 #pragma unroll
-        for (int h = 0; h < 8; ++h)  // padding slots are not read
-          if (8 * q + h < cnt) sum += yr[(h & 1) ? (wv[h >> 1] >> 16) : (wv[h >> 1] & 0xFFFFu)];
+        for (int h = 0; h < 8; ++h)
+          if (8 * q + h < steps) sum += yr[(h & 1) ? (wv[h >> 1] >> 16) : (wv[h >> 1] & 0xFFFFu)];
       }
       const int32_t g = code & 0x3FFFFFFF;
       if (code & 0x40000000) dst[g] = sum;

@@ -122,8 +122,8 @@ class CGOperator final : public Operator {
   }
 
   // cube-block tables of cg_cube_kernel (blocks of 64 hexes = 384 tets)
-  DevBuf<int16_t> d_tmapv, d_cslot8;
-  DevBuf<uint32_t> d_ritem;
+  DevBuf<int16_t> d_tmapv, d_cslot8[3];
+  DevBuf<uint32_t> d_ritem[3];
   DevBuf<int32_t> d_bdof;
   int64_t n_blocks = 0;
   int cube_NB = 0;
@@ -240,35 +240,125 @@ class CGOperator final : public Operator {
     // lane:
     //   tmapv  [KV/8][384] x 8 int16: slot of tet t's local DoF i (KV = K
     //          rounded up to 8, padding entries 0);
-    //   cslot8 per warp-round, [groups][32 lanes] x 8 int16: contributing row
-    //          slots (t' * KP + i) of each slot, padded with the zero slot
-    //          384 * KP (not read);
-    //   ritem  [NB]: contributions | (first cslot8 entry << 8).
-    const int KV = (K + 7) / 8 * 8, ZERO = 384 * KP;
+    //   cslot8 per warp-round, [groups][32 lanes] x 8 int16: the row slot
+    //          (t' * KP + i) each lane reads at each step;
+    //   ritem  [NB]: steps of the lane | (first cslot8 entry << 8).
+    // Three reduce schedules (kernel variants 5, 6, 7):
+    //   0  each lane reads its contributions in (tet, local DoF) order;
+    //   1  bank-scheduled, the same steps for every lane of a warp-round;
+    //   2  bank-scheduled, each lane stops after its last contribution.
+    // Bank-scheduled steps come from an edge colouring of the bipartite
+    // multigraph lanes x shared-memory banks (one edge per contribution): a
+    // bipartite multigraph of maximum degree D has a proper D-edge-colouring
+    // (Konig), found here by alternating-path recolouring.  Colour = step, so
+    // no two lanes of one step hit the same bank and every step is one
+    // shared-memory wavefront (per half-warp for 8-byte values).  A lane with
+    // nothing to add at a step reads one of the zero slots 384 * KP + z (one
+    // per bank), in a bank that no other lane of the step uses.
+    const int KV = (K + 7) / 8 * 8;
     std::vector<int16_t> tmv(size_t(384) * KV, 0);
     for (int t = 0; t < 384; ++t)
       for (int i = 0; i < K; ++i) tmv[(size_t(i / 8) * 384 + t) * 8 + i % 8] = int16_t(slot_of[tm0[t * K + i]]);
-    std::vector<int16_t> c8;
-    std::vector<uint32_t> items(NB);
-    for (int n0 = 0; n0 < NB; n0 += 32) {
-      const int len = std::min(32, NB - n0);
-      size_t mx = 0;
-      for (int l = 0; l < len; ++l) mx = std::max(mx, contrib[dof_at[n0 + l]].size());
-      const size_t e0 = c8.size() / 8;
-      c8.resize(c8.size() + (mx + 7) / 8 * 32 * 8, int16_t(ZERO));
-      for (int l = 0; l < len; ++l) {
-        const std::vector<int16_t>& cl = contrib[dof_at[n0 + l]];
-        SFEM_REQUIRE(!cl.empty() && cl.size() < 256, FEM_ERR_INTERNAL,
-                     "cube tables: contribution count out of range");
-        for (size_t e = 0; e < cl.size(); ++e) c8[((e0 + e / 8 * 32) + l) * 8 + e % 8] = cl[e];
-        items[n0 + l] = uint32_t(cl.size()) | (uint32_t(e0 + l) << 8);
+    const int nbank = sizeof(T) == 8 ? 16 : 32;  // 8-byte values: 16 bank pairs per half-warp
+    const int span = sizeof(T) == 8 ? 16 : 32;   // lanes that share one wavefront
+    SFEM_REQUIRE(384 * KP + 32 < 32768, FEM_ERR_INTERNAL, "cube tables exceed their index bits");
+    for (int mode = 0; mode < 3; ++mode) {
+      std::vector<int16_t> c8;
+      std::vector<uint32_t> items(NB);
+      for (int n0 = 0; n0 < NB; n0 += 32) {
+        const int len = std::min(32, NB - n0);
+        std::vector<std::vector<int>> step_slot(32);  // per lane: slot at each step, -1 = none
+        for (int h0 = 0; h0 < len; h0 += span) {
+          const int h1 = std::min(len, h0 + span);
+          if (mode == 0) {
+            for (int l = h0; l < h1; ++l)
+              for (int16_t v : contrib[dof_at[n0 + l]]) step_slot[l].push_back(v);
+            continue;
+          }
+          std::vector<std::pair<int, int>> edges;  // (lane in span, slot)
+          std::vector<int> degl(span, 0), degb(nbank, 0);
+          for (int l = h0; l < h1; ++l)
+            for (int16_t v : contrib[dof_at[n0 + l]]) {
+              edges.emplace_back(l - h0, v);
+              ++degl[l - h0];
+              ++degb[v % nbank];
+            }
+          const int D = std::max(*std::max_element(degl.begin(), degl.end()),
+                                 *std::max_element(degb.begin(), degb.end()));
+          std::vector<int> Lc(size_t(span) * D, -1), Bc(size_t(nbank) * D, -1), col(edges.size(), -1);
+          auto lc = [&](int u, int c) -> int& { return Lc[size_t(u) * D + c]; };
+          auto bc = [&](int v, int c) -> int& { return Bc[size_t(v) * D + c]; };
+          for (size_t e = 0; e < edges.size(); ++e) {
+            const int u = edges[e].first, v = edges[e].second % nbank;
+            int a = 0, c2 = 0;
+            while (lc(u, a) >= 0) ++a;
+            while (bc(v, c2) >= 0) ++c2;
+            if (a != c2 && bc(v, a) >= 0) {
+              // swap colours a and c2 along the alternating path that leaves bank v by colour a
+              std::vector<int> path;
+              bool at_bank = true;
+              int node = v, c = a;
+              for (;;) {
+                const int ed = at_bank ? bc(node, c) : lc(node, c);
+                if (ed < 0) break;
+                path.push_back(ed);
+                node = at_bank ? edges[ed].first : edges[ed].second % nbank;
+                at_bank = !at_bank;
+                c = c == a ? c2 : a;
+              }
+              for (int ed : path) {
+                lc(edges[ed].first, col[ed]) = -1;
+                bc(edges[ed].second % nbank, col[ed]) = -1;
+              }
+              for (int ed : path) {
+                col[ed] = col[ed] == a ? c2 : a;
+                lc(edges[ed].first, col[ed]) = ed;
+                bc(edges[ed].second % nbank, col[ed]) = ed;
+              }
+            }
+            SFEM_REQUIRE(lc(u, a) < 0 && bc(v, a) < 0, FEM_ERR_INTERNAL, "cube tables: edge colouring failed");
+            col[e] = a;
+            lc(u, a) = int(e);
+            bc(v, a) = int(e);
+          }
+          for (size_t e = 0; e < edges.size(); ++e) {
+            std::vector<int>& st = step_slot[h0 + edges[e].first];
+            if (int(st.size()) <= col[e]) st.resize(col[e] + 1, -1);
+            st[col[e]] = edges[e].second;
+          }
+        }
+        int S = 0;
+        for (int l = 0; l < len; ++l) S = std::max(S, int(step_slot[l].size()));
+        SFEM_REQUIRE(S > 0 && S < 256, FEM_ERR_INTERNAL, "cube tables: step count out of range");
+        std::vector<int> steps(len);
+        for (int l = 0; l < len; ++l) {
+          steps[l] = mode == 1 ? S : int(step_slot[l].size());
+          step_slot[l].resize(S, -1);
+        }
+        // gaps: a zero slot in a bank that no lane of the span reads at that step
+        for (int h0 = 0; h0 < len; h0 += span) {
+          const int h1 = std::min(len, h0 + span);
+          for (int st = 0; st < S; ++st) {
+            std::vector<char> busy(nbank, 0);
+            for (int l = h0; l < h1; ++l)
+              if (step_slot[l][st] >= 0) busy[step_slot[l][st] % nbank] = 1;
+            const int f = int(std::find(busy.begin(), busy.end(), 0) - busy.begin());
+            for (int l = h0; l < h1; ++l)
+              if (step_slot[l][st] < 0) step_slot[l][st] = 384 * KP + ((f % nbank - 384 * KP) % nbank + nbank) % nbank;
+          }
+        }
+        const size_t e0 = c8.size() / 8;
+        c8.resize(c8.size() + size_t((S + 7) / 8) * 32 * 8, int16_t(384 * KP));
+        for (int l = 0; l < len; ++l) {
+          for (int e = 0; e < S; ++e) c8[((e0 + size_t(e / 8) * 32) + l) * 8 + e % 8] = int16_t(step_slot[l][e]);
+          items[n0 + l] = uint32_t(steps[l]) | (uint32_t(e0 + l) << 8);
+        }
       }
+      SFEM_REQUIRE(c8.size() / 8 < (size_t(1) << 24), FEM_ERR_INTERNAL, "cube tables exceed their index bits");
+      d_ritem[mode].upload(items);
+      d_cslot8[mode].upload(c8);
     }
-    SFEM_REQUIRE(ZERO < 32768 && c8.size() / 8 < (size_t(1) << 24), FEM_ERR_INTERNAL,
-                 "cube tables exceed their index bits");
     d_tmapv.upload(tmv);
-    d_ritem.upload(items);
-    d_cslot8.upload(c8);
     d_bdof.upload(bd);
     n_blocks = nbk;
     cube_NB = NB;
@@ -287,7 +377,7 @@ class CGOperator final : public Operator {
 
   int cube_grid = 0;
   template <int P, int NB, int KP>
-  static size_t cube_smem() { return (2 * size_t(NB) + 384 * size_t(KP) + 1) * sizeof(T); }
+  static size_t cube_smem() { return (2 * size_t(NB) + 384 * size_t(KP) + (sizeof(T) == 8 ? 16 : 32)) * sizeof(T); }
   template <int P, int NB, int KP>
   void setup_cube() {
     auto kern = cg_cube_pipe_kernel<P, T, NB, KP>;
@@ -300,9 +390,9 @@ class CGOperator final : public Operator {
     cube_grid = int(std::min<int64_t>(n_blocks, int64_t(sms) * occ));
   }
   template <int P, int NB, int KP>
-  void launch_cube(const T* x, T* d, cudaStream_t s) {
+  void launch_cube(const T* x, T* d, int sched, cudaStream_t s) {
     cg_cube_pipe_kernel<P, T, NB, KP><<<unsigned(cube_grid), 384, cube_smem<P, NB, KP>(), s>>>(
-        n_blocks, d_tmapv.p, d_bdof.p, d_ritem.p, d_cslot8.p, d_geo.p, x, d, d_constrained.n,
+        n_blocks, d_tmapv.p, d_bdof.p, d_ritem[sched].p, d_cslot8[sched].p, d_geo.p, x, d, d_constrained.n,
         d_constrained.p);
   }
 
@@ -462,11 +552,16 @@ class CGOperator final : public Operator {
       if (v == 3 && n_blocks < kFill) v = 2;
       if (v == 2 && n_hex < kFill * kHexBS) v = 1;
     }
+    // cube reduce schedule: variants 5, 6, 7 pick one; variant 3 takes the
+    // one measured fastest on B200 (FP64 P2: bank-scheduled with uniform
+    // steps, 398 against 415 us on 128^3; all others: contribution order)
+    int sched = v >= 5 ? v - 5 : (sizeof(T) == 8 && cfg.degree == 2 ? 1 : 0);
+    if (v >= 5) v = 3;
     if (v == 3 && cube_NB) {
       switch (cfg.degree) {
-        case 1: launch_cube<1, 125, 5>(x, d, s); break;
-        case 2: launch_cube<2, 729, 11>(x, d, s); break;
-        case 3: launch_cube<3, 2197, 21>(x, d, s); break;
+        case 1: launch_cube<1, 125, 5>(x, d, sched, s); break;
+        case 2: launch_cube<2, 729, 11>(x, d, sched, s); break;
+        case 3: launch_cube<3, 2197, 21>(x, d, sched, s); break;
       }
       SFEM_CUDA(cudaGetLastError());
       return;

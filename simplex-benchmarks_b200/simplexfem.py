@@ -373,7 +373,7 @@ class Batch:
 
 def _autotune(fn, handle, reps, use_cache):
     v, c = C.c_int32(), C.c_int32()
-    us = (C.c_double * 5)()
+    us = (C.c_double * 8)()
     check(fn(handle, reps, int(bool(use_cache)), C.byref(v), C.byref(c), us))
     return {"variant": v.value, "cached": bool(c.value), "us": list(us)}
 
