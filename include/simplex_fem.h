@@ -142,6 +142,18 @@ int fem_op_copy_support_points(const fem_op* op, double* xyz /* [m/n_components]
  * (CG/cells_batched/application.cc:1167-1176, DG/cells_batched/application.cc:1319-1332,
  * application_helmholtz.cc:567-580): dst = A src.  dst and src must not alias. */
 int fem_op_vmult(fem_op* op, void* dst, const void* src, void* stream);
+/* dst_host[i] = A src_host[i] for i < n, on vectors in HOST memory (the
+ * reference's Operator::vmult on deal.II host vectors,
+ * CG/cells_batched/application.cc:1154-1176, DG/cells_batched/
+ * application.cc:1303-1316): each src is copied to the device, the operator
+ * applied and dst copied back.  Enqueued on `stream` (asynchronous: the host
+ * buffers must stay valid, and dst is ready, when the stream passes the
+ * call).  The operator keeps two device staging pairs (4 x m values, made by
+ * the first call) and its own copy-in, compute and copy-out streams, so with
+ * pinned host memory the copy-in of vector i+1, the apply of vector i and the
+ * copy-out of vector i-1 overlap.  Pageable host memory works, with copies
+ * that do not overlap. */
+int fem_op_vmult_host(fem_op* op, int32_t n, void* const* dst_host, const void* const* src_host, void* stream);
 /* Same product as fem_op_vmult for FEM_DG / FEM_HELMHOLTZ operators, for
  * callers that must not allocate device memory at the call (their memory
  * pool owns the device, or cudaMalloc's implicit synchronisation and

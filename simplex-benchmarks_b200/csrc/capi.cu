@@ -7,6 +7,7 @@
 #include "../../include/simplex_fem.h"
 #include "common.hpp"
 #include "autotune.hpp"
+#include "host_vmult.hpp"
 #include "handles.hpp"
 
 namespace sfem {
@@ -231,6 +232,15 @@ int fem_op_compute_diagonal(fem_op* op, void* diag, void* stream) {
     REQUIRE_PTR(op);
     REQUIRE_PTR(diag);
     op->op->diagonal(diag, static_cast<cudaStream_t>(stream));
+  });
+}
+
+int fem_op_vmult_host(fem_op* op, int32_t n, void* const* dst_host, const void* const* src_host, void* stream) {
+  return guarded([&] {
+    REQUIRE_PTR(op);
+    REQUIRE_PTR(dst_host);
+    REQUIRE_PTR(src_host);
+    sfem::vmult_host(*op->op, n, dst_host, src_host, static_cast<cudaStream_t>(stream));
   });
 }
 

@@ -64,9 +64,12 @@ struct OpConfig {
   int kernel_variant = 0;  // 0: tuned default (see fem_op_params.kernel_variant)
 };
 
+struct HostPipe;  // staging buffers and streams of vmult_host (host_vmult.cu)
+
 class Operator {
  public:
   virtual ~Operator() = default;
+  std::shared_ptr<HostPipe> host_pipe;  // created by the first vmult_host
   OpConfig cfg;
   const Mesh* mesh = nullptr;  // the mesh the operator was built on (must outlive it)
   int K = 0;               // DoFs per cell and component

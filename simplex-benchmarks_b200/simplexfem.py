@@ -103,6 +103,7 @@ _PROTOS = [
     ("fem_op_compute_inverse_diagonal", C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p]),
     ("fem_op_compute_diagonal", C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p]),
     ("fem_op_set_kernel_variant", C.c_int, [C.c_void_p, C.c_int32]),
+    ("fem_op_vmult_host", C.c_int, [C.c_void_p, C.c_int32, C.c_void_p, C.c_void_p, C.c_void_p]),
     ("fem_op_work", C.c_int, [C.c_void_p, C.POINTER(C.c_double), C.POINTER(C.c_double)]),
     ("fem_op_status", C.c_int, [C.c_void_p, C.POINTER(C.c_int32)]),
     ("fem_op_rhs", C.c_int, [C.c_void_p, C.POINTER(RhsDesc), C.c_void_p, C.c_void_p]),
@@ -280,6 +281,20 @@ class Operator:
         self._check_vec(dst)
         self._check_vec(src)
         check(lib().fem_op_vmult(self.handle, _ptr(dst), _ptr(src), _stream_ptr(stream)))
+
+    def vmult_host(self, dsts, srcs, stream=None):
+        """dsts[i] = A srcs[i] on vectors in host memory (fem_op_vmult_host):
+        CPU tensors of the operator's dtype and length m (pinned memory lets
+        the copies of consecutive vectors overlap).  Asynchronous on `stream`."""
+        if len(dsts) != len(srcs) or not dsts:
+            raise ValueError("vmult_host needs equal, non-empty lists of dst and src vectors")
+        for v in list(dsts) + list(srcs):
+            if v.device.type != "cpu" or v.dtype != self.dtype or v.numel() != self.m() or not v.is_contiguous():
+                raise ValueError("vmult_host vectors must be contiguous CPU tensors of the operator's dtype and length")
+        n = len(dsts)
+        da = (C.c_void_p * n)(*[d.data_ptr() for d in dsts])
+        sa = (C.c_void_p * n)(*[s.data_ptr() for s in srcs])
+        check(lib().fem_op_vmult_host(self.handle, n, da, sa, _stream_ptr(stream)))
 
     def vmult_phase(self, dst, src, phase, stream=None):
         self._check_vec(dst)
