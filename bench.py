@@ -155,18 +155,20 @@ class ClockSampler:
 
 
 def timed_steps(fn, steps, warmup, stream, flush=None):
-    """Per-step device time (ms) of fn() with CUDA events on `stream`."""
+    """Per-step device time (ms) of fn() with CUDA events on `stream`; flush(s)
+    writes the L2-sized buffer on stream s, the timing stream, so that it ends
+    before the timed work starts."""
     import torch
     for _ in range(warmup):
         if flush:
-            flush()
+            flush(stream)
         fn()
     torch.cuda.synchronize()
     ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(steps)]
     with torch.cuda.stream(stream):
         for a, b in ev:
             if flush:
-                flush()
+                flush(stream)
             a.record(stream)
             fn()
             b.record(stream)
@@ -462,8 +464,8 @@ def run_ours(args):
     stream = torch.cuda.Stream()
     flush_buf = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")
 
-    def flush():
-        with torch.cuda.stream(stream):
+    def flush(on):
+        with torch.cuda.stream(on):
             flush_buf.fill_(1.0)
 
     mesh, op, x = build_problem("fp64")
