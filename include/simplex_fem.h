@@ -87,14 +87,15 @@ typedef struct fem_op_params {
                               cell, 2 thread per Kuhn hex (6 tets, one atomic per distinct
                               DoF), 3 CTA per 4x4x4-hex Morton cube (stores for cube-interior
                               DoFs); each falls back to the next simpler form where the mesh
-                              lacks the pattern; default P1 2, P2 3, P3 3 (FP32) / 1 (FP64);
+                              lacks the pattern; default P1 3 (FP64) / 2 (FP32), P2 3, P3 3
+                              (FP32) / 1 (FP64);
                               4: FP32 CG on the TF32 tensor cores (tcgen05 kind::tf32, cell
                               operator as one [128 cells x K] x [K x 6K] product; ~1e-3
                               relative accuracy, for multigrid levels); CG 5, 6, 7: the cube
                               kernel (3) with its DoF reduction read in contribution order
                               (5), bank-scheduled with the same steps per warp (6) or
                               bank-scheduled with per-lane steps (7); 3 takes the fastest
-                              measured on B200 (6 for FP64 P2, else 5) */
+                              measured on B200 (6 for FP64 P1 and P2, else 5) */
   int32_t reserved[5];
 } fem_op_params;
 

@@ -176,8 +176,21 @@ __global__ void __launch_bounds__(BS) cg_hex_kernel(int64_t n_hex, const int32_t
 // loaded into registers, and the atomics of cube k-1 drain.  Buffer reuse is
 // ordered by the two block barriers of every iteration (a buffer is refilled
 // only after the barrier that follows its last read).
-// Shared memory: (2 NB + 384 KP + NZ) values, NZ = 16 zero slots for 8-byte
-// values (bank pairs), 32 for 4-byte values.
+// The tet metric of the next cube arrives one of two ways (cube_metric_smem):
+// loaded into registers one cube ahead, or streamed into shared memory with
+// 16-byte cp.async copies issued after the apply of the current cube (its six
+// [384] rows are contiguous in geo), landing during the reduction.  The second
+// frees the prefetch registers but takes 6 x 384 values of shared memory, which
+// the L1 cache loses: measured on B200 it is faster for P3 FP32 (130 against
+// 136 us on 64^3) and P1 FP64 (155 against 177 us on 128^3), slower for P2
+// FP64 (421 against 396 us) and P3 FP64, even for P2 FP32.
+// Shared memory: ((6 x 384) + 2 NB + 384 KP + NZ) values, NZ = 16 zero slots
+// for 8-byte values (bank pairs), 32 for 4-byte values.
+template <int P, typename T>
+__host__ __device__ constexpr bool cube_metric_smem() {
+  return (P == 3 && sizeof(T) == 4) || (P == 1 && sizeof(T) == 8);
+}
+
 template <int P, typename T, int NB, int KP>
 __global__ void __launch_bounds__(384, P <= 2 ? 3 : (sizeof(T) == 4 ? 2 : 1))
     cg_cube_pipe_kernel(int64_t n_blocks, const int16_t* __restrict__ tmapv, const int32_t* __restrict__ bdof,
@@ -187,9 +200,11 @@ __global__ void __launch_bounds__(384, P <= 2 ? 3 : (sizeof(T) == 4 ? 2 : 1))
   constexpr int K = O::K;
   constexpr int KV = (K + 7) / 8 * 8;
   constexpr int NJ = (NB + 383) / 384;  // cube DoFs gathered per thread
+  constexpr bool GS = cube_metric_smem<P, T>();
   extern __shared__ __align__(16) unsigned char smem_cube[];
-  T* ubuf = reinterpret_cast<T*>(smem_cube);  // [2][NB]
-  T* yr = ubuf + 2 * NB;                      // [384][KP], then the zero slots
+  T* sg = reinterpret_cast<T*>(smem_cube);  // GS: [6][384] metric of the cube
+  T* ubuf = sg + (GS ? 6 * 384 : 0);        // [2][NB]
+  T* yr = ubuf + 2 * NB;                    // [384][KP], then the zero slots
   const int t = threadIdx.x;
   if (t < (sizeof(T) == 8 ? 16 : 32)) yr[384 * KP + t] = T(0);
   const int64_t stride = gridDim.x;
@@ -223,30 +238,48 @@ __global__ void __launch_bounds__(384, P <= 2 ? 3 : (sizeof(T) == 4 ? 2 : 1))
     }
     asm volatile("cp.async.commit_group;" ::: "memory");
   };
-  auto load_geo = [&](int64_t b, T (&G)[6]) {
+  // GS: cp.async (16 bytes, L2 only) of cube bq's metric rows into sg
+  auto issue_geo = [&](int64_t bq) {
+    constexpr int CH = 384 * int(sizeof(T)) / 16;  // 16-byte chunks per row
+    if (GS && bq < n_blocks)
+      for (int e = t; e < 6 * CH; e += 384) {
+        const int k = e / CH, ch = e % CH;
+        const uint32_t sa = static_cast<uint32_t>(__cvta_generic_to_shared(sg + k * 384 + ch * (16 / sizeof(T))));
+        asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(sa),
+                     "l"(geo + k * n_cells + bq * 384 + ch * (16 / int(sizeof(T))))
+                     : "memory");
+      }
+    asm volatile("cp.async.commit_group;" ::: "memory");
+  };
+  // !GS: the metric of cube bq into registers
+  auto load_geo = [&](int64_t bq, T (&G)[6]) {
 #pragma unroll
-    for (int k = 0; k < 6; ++k) G[k] = b < n_blocks ? __ldg(geo + k * n_cells + b * 384 + t) : T(0);
+    for (int k = 0; k < 6; ++k) G[k] = bq < n_blocks ? __ldg(geo + k * n_cells + bq * 384 + t) : T(0);
   };
 
   int64_t b = blockIdx.x;
   int32_t code_cur[NJ], code_nxt[NJ];
-  T G[6], Gn[6];
+  T Gc[6], Gn[6];
   load_codes(b, code_cur);
   issue_gather(code_cur, 0, b < n_blocks);
+  if (GS) issue_geo(b);
+  else load_geo(b, Gc);
   load_codes(b + stride, code_nxt);
-  load_geo(b, G);
   for (int k = 0; b < n_blocks; ++k, b += stride) {
     const int buf = k & 1;
     const bool more = b + stride < n_blocks;
-    // gather of the next cube, codes of the one after, metric of the next
+    // gather of the next cube, codes of the one after (and !GS: metric of the next)
     issue_gather(code_nxt, buf ^ 1, more);
 #pragma unroll
     for (int q = 0; q < NJ; ++q) code_cur[q] = code_nxt[q];
     load_codes(b + 2 * stride, code_nxt);
-    load_geo(b + stride, Gn);
-    asm volatile("cp.async.wait_group 1;" ::: "memory");  // this cube's gather
+    if (!GS) load_geo(b + stride, Gn);
+    asm volatile("cp.async.wait_group 1;" ::: "memory");  // this cube's gather (GS: and metric)
     __syncthreads();
     {
+      T G[6];
+#pragma unroll
+      for (int k6 = 0; k6 < 6; ++k6) G[k6] = GS ? sg[k6 * 384 + t] : Gc[k6];
       const T* ub = ubuf + buf * NB;
       const uint4* tm = reinterpret_cast<const uint4*>(tmapv) + t;
       int ti[KV];
@@ -268,6 +301,7 @@ __global__ void __launch_bounds__(384, P <= 2 ? 3 : (sizeof(T) == 4 ? 2 : 1))
       for (int i = 0; i < K; ++i) yr[t * KP + i] = yt[i];
     }
     __syncthreads();
+    if (GS) issue_geo(b + stride);  // every thread has read this cube's metric
     const int32_t* bd = bdof + b * NB;
 #pragma unroll 1
     for (int r = 0; r < NJ; ++r) {
@@ -290,8 +324,10 @@ __global__ void __launch_bounds__(384, P <= 2 ? 3 : (sizeof(T) == 4 ? 2 : 1))
       if (code & 0x40000000) dst[g] = sum;
       else atomicAdd(dst + g, sum);
     }
+    if (!GS) {
 #pragma unroll
-    for (int k6 = 0; k6 < 6; ++k6) G[k6] = Gn[k6];
+      for (int k6 = 0; k6 < 6; ++k6) Gc[k6] = Gn[k6];
+    }
   }
   asm volatile("cp.async.wait_group 0;" ::: "memory");
 }

@@ -377,7 +377,10 @@ class CGOperator final : public Operator {
 
   int cube_grid = 0;
   template <int P, int NB, int KP>
-  static size_t cube_smem() { return (2 * size_t(NB) + 384 * size_t(KP) + (sizeof(T) == 8 ? 16 : 32)) * sizeof(T); }
+  static size_t cube_smem() {
+    return ((cube_metric_smem<P, T>() ? 6 * 384 : 0) + 2 * size_t(NB) + 384 * size_t(KP) + (sizeof(T) == 8 ? 16 : 32)) *
+           sizeof(T);
+  }
   template <int P, int NB, int KP>
   void setup_cube() {
     auto kern = cg_cube_pipe_kernel<P, T, NB, KP>;
@@ -536,8 +539,8 @@ class CGOperator final : public Operator {
       SFEM_CUDA(cudaMemsetAsync(d, 0, sizeof(T) * m, s));
       return;
     }
-    // default (variant 0), measured on B200: P1 per hex, P2 per cube, P3 per
-    // cube in FP32 and per cell in FP64; per cell on meshes too small to give
+    // default (variant 0), measured on B200: P1 per cube in FP64 and per hex
+    // in FP32, P2 per cube, P3 per cube in FP32 and per cell in FP64; per cell on meshes too small to give
     // every SM two cubes (or two CTAs of hexes), where the coarser forms
     // leave SMs idle
     int v = cfg.kernel_variant;
@@ -548,14 +551,15 @@ class CGOperator final : public Operator {
     }
     if (v == 0) {
       constexpr int64_t kFill = 2 * 148;
-      v = cfg.degree == 1 ? 2 : cfg.degree == 2 ? 3 : (sizeof(T) == 4 ? 3 : 1);
+      v = cfg.degree == 1 ? (sizeof(T) == 8 ? 3 : 2) : cfg.degree == 2 ? 3 : (sizeof(T) == 4 ? 3 : 1);
       if (v == 3 && n_blocks < kFill) v = 2;
       if (v == 2 && n_hex < kFill * kHexBS) v = 1;
     }
     // cube reduce schedule: variants 5, 6, 7 pick one; variant 3 takes the
-    // one measured fastest on B200 (FP64 P2: bank-scheduled with uniform
-    // steps, 398 against 415 us on 128^3; all others: contribution order)
-    int sched = v >= 5 ? v - 5 : (sizeof(T) == 8 && cfg.degree == 2 ? 1 : 0);
+    // one measured fastest on B200 (FP64 P1 and P2: bank-scheduled with
+    // uniform steps, 155 against 165 us and 396 against 415 us on 128^3;
+    // FP32: contribution order)
+    int sched = v >= 5 ? v - 5 : (sizeof(T) == 8 && cfg.degree <= 2 ? 1 : 0);
     if (v >= 5) v = 3;
     if (v == 3 && cube_NB) {
       switch (cfg.degree) {
