@@ -311,7 +311,7 @@ __global__ void __launch_bounds__(384, P <= 2 ? 3 : (sizeof(T) == 4 ? 2 : 1))
       if (code < 0) continue;
       const uint32_t item = __ldg(ritem + n);
       const uint4* grp = reinterpret_cast<const uint4*>(cslot8) + (item >> 8);
-      const int steps = int(item & 0xFFu);  // the same for every lane of the warp
+      const int steps = int(item & 0xFFu);  // per lane; the same for every lane in schedule 1
       T sum = T(0);
       for (int q = 0; 8 * q < steps; ++q) {
         const uint4 w = __ldg(grp + 32 * q);
