@@ -219,7 +219,8 @@ def mg_solve_bench(repeats=5, learned=True):
     """Poisson solve to rel. residual 1e-8: CG P3 on 64^3 x 6 tets (7,189,057 DoFs),
     f = sum of 8 sin(k.x), k ~ U[1,6]^3 (PCG64 seed 2); FP64 outer CG preconditioned by
     the hybrid p(3-2-1)/h(64-32-16-8-4) multigrid with Chebyshev(3)-Jacobi smoothing and a
-    CUDA-graph V-cycle; levels in FP32 (mixed) vs FP64."""
+    CUDA-graph V-cycle; levels in FP32 (mixed; CUDA-core, and TF32 tensor-core
+    contractions for the CG levels) vs FP64."""
     import torch
     import simplexfem as sf
     mesh = sf.Mesh(64)
@@ -228,8 +229,8 @@ def mg_solve_bench(repeats=5, learned=True):
     x = op.initialize_dof_vector()
     out = {"workload": "CG P3 Poisson, 64^3 x 6 Kuhn tets, 7,189,057 DoFs, rel. residual 1e-8",
            "dofs": op.m()}
-    for prec in ("fp64", "fp32"):
-        mg = sf.Multigrid(op, precision=prec, smoother_degree=3)
+    for prec, tc in (("fp64", False), ("fp32", False), ("fp32", True)):
+        mg = sf.Multigrid(op, precision=prec, smoother_degree=3, tensor_cores=tc)
         cg = sf.SolverCG(op, mg)
         cg.solve(x, b, rtol=1e-8)  # warm-up (graph capture)
         times, its = [], None
@@ -242,7 +243,7 @@ def mg_solve_bench(repeats=5, learned=True):
             times.append(time.perf_counter() - t0)
             its = r["iterations"]
             assert r["status"] == 0
-        key = "fp64_mg" if prec == "fp64" else "mixed_mg"
+        key = "fp64_mg" if prec == "fp64" else ("mixed_tf32_mg" if tc else "mixed_mg")
         out[key] = {"ms": 1e3 * min(times), "ms_median": 1e3 * statistics.median(times), "iterations": its,
                     "dofs_per_s": op.m() / min(times)}
         del cg, mg

@@ -95,7 +95,10 @@ typedef struct fem_op_params {
                               kernel (3) with its DoF reduction read in contribution order
                               (5), bank-scheduled with the same steps per warp (6) or
                               bank-scheduled with per-lane steps (7); 3 takes the fastest
-                              measured on B200 (6 for FP64 P1 and P2, else 5) */
+                              measured on B200 (6 for FP64 P1 and P2, else 5); CG 8:
+                              FP32 on the TF32 tensor cores per cube (the cube kernel
+                              with each tile of 128 tets as one tcgen05 product;
+                              variant 4 on meshes without whole cubes) */
   int32_t reserved[5];
 } fem_op_params;
 
@@ -232,7 +235,8 @@ typedef struct fem_mg_params {
                                (cph / chp; DG/cells_batched/application_phc.cc:3396-3652) */
   int32_t learned_steps;    /* learned finest-level smoothing per V-cycle: 1 pre, 2 post, 3 both (3) */
   int32_t tensor_cores;     /* FP32 CG levels apply their operator with TF32 tensor-core
-                               contractions (kernel variant 4; operator accurate to ~1e-3) */
+                               contractions (kernel variant 8: per cube, or per cell on
+                               levels without whole cubes; operator accurate to ~1e-3) */
   int32_t reserved[1];
 } fem_mg_params;
 int fem_mg_params_default(fem_mg_params* p);

@@ -146,6 +146,37 @@ __global__ void __launch_bounds__(BS) cg_hex_kernel(int64_t n_hex, const int32_t
   }
 }
 
+// DoF reduction of one cube (cube kernels): thread t sums the contributions of
+// its reduce slots n = 384 r + t from the per-tet result rows yr, in the order
+// of its cslot8 steps, and writes each DoF once (store for cube-interior DoFs,
+// atomic on the cube surface).  bd: the cube's row of bdof.
+template <typename T, int NB>
+__device__ __forceinline__ void cube_reduce(int t, const int32_t* __restrict__ bd, const uint32_t* __restrict__ ritem,
+                                            const int16_t* __restrict__ cslot8, const T* yr, T* __restrict__ dst) {
+  constexpr int NJ = (NB + 383) / 384;
+#pragma unroll 1
+  for (int r = 0; r < NJ; ++r) {
+    const int n = 384 * r + t;
+    if (n >= NB) break;
+    const int32_t code = __ldg(bd + n);
+    if (code < 0) continue;
+    const uint32_t item = __ldg(ritem + n);
+    const uint4* grp = reinterpret_cast<const uint4*>(cslot8) + (item >> 8);
+    const int steps = int(item & 0xFFu);  // per lane; the same for every lane in schedule 1
+    T sum = T(0);
+    for (int q = 0; 8 * q < steps; ++q) {
+      const uint4 w = __ldg(grp + 32 * q);
+      const uint32_t wv[4] = {w.x, w.y, w.z, w.w};
+#pragma unroll
+      for (int h = 0; h < 8; ++h)
+        if (8 * q + h < steps) sum += yr[(h & 1) ? (wv[h >> 1] >> 16) : (wv[h >> 1] & 0xFFFFu)];
+    }
+    const int32_t g = code & 0x3FFFFFFF;
+    if (code & 0x40000000) dst[g] = sum;
+    else atomicAdd(dst + g, sum);
+  }
+}
+
 // Cube-block form for Kuhn meshes whose hexes come in Morton order: 64
 // consecutive hexes (384 tets) form a 4 x 4 x 4 cube, and every cube has the
 // same local structure, so one set of small tables serves all cubes.  One
@@ -302,28 +333,7 @@ __global__ void __launch_bounds__(384, P <= 2 ? 3 : (sizeof(T) == 4 ? 2 : 1))
     }
     __syncthreads();
     if (GS) issue_geo(b + stride);  // every thread has read this cube's metric
-    const int32_t* bd = bdof + b * NB;
-#pragma unroll 1
-    for (int r = 0; r < NJ; ++r) {
-      const int n = 384 * r + t;
-      if (n >= NB) break;
-      const int32_t code = __ldg(bd + n);
-      if (code < 0) continue;
-      const uint32_t item = __ldg(ritem + n);
-      const uint4* grp = reinterpret_cast<const uint4*>(cslot8) + (item >> 8);
-      const int steps = int(item & 0xFFu);  // per lane; the same for every lane in schedule 1
-      T sum = T(0);
-      for (int q = 0; 8 * q < steps; ++q) {
-        const uint4 w = __ldg(grp + 32 * q);
-        const uint32_t wv[4] = {w.x, w.y, w.z, w.w};
-#pragma unroll
-        for (int h = 0; h < 8; ++h)
-          if (8 * q + h < steps) sum += yr[(h & 1) ? (wv[h >> 1] >> 16) : (wv[h >> 1] & 0xFFFFu)];
-      }
-      const int32_t g = code & 0x3FFFFFFF;
-      if (code & 0x40000000) dst[g] = sum;
-      else atomicAdd(dst + g, sum);
-    }
+    cube_reduce<T, NB>(t, bdof + b * NB, ritem, cslot8, yr, dst);
     if (!GS) {
 #pragma unroll
       for (int k6 = 0; k6 < 6; ++k6) Gc[k6] = Gn[k6];

@@ -527,7 +527,7 @@ class MultigridImpl final : public Multigrid {
       L.hexes = L.mesh->desc.n[0];
       cfg.degree = L.degree;
       cfg.kind = L.kind;
-      cfg.kernel_variant = prm.tensor_cores && L.kind == FEM_CG && cfg.precision == FEM_FP32 ? 4 : 0;
+      cfg.kernel_variant = prm.tensor_cores && L.kind == FEM_CG && cfg.precision == FEM_FP32 ? 8 : 0;
       L.op = make_operator(*L.mesh, cfg);
       const int64_t m = L.op->m;
       L.inv_diag.alloc(m);

@@ -76,33 +76,39 @@ class CGOperator final : public Operator {
   DevBuf<int> d_status;
   int tc_grid = 0;
 
+  // (S_c)_ij of the cell operator y = sum_c G_c S_c u over the metric
+  // components c = (00,11,22,01,02,12): S_aa = D_a^T MQ D_a,
+  // S_ab = D_a^T MQ D_b + D_b^T MQ D_a
   template <int P>
-  void build_tc_tables() {
+  static double stiffness_S(int c, int i, int j) {
     using Tb = ref::Tables<P>;
-    using Sh = CGTcShape<P>;
     constexpr int KQ = Tb::KQ;
-    // E_ab = D_a^T MQ D_b, [K][K]
-    auto E = [&](int a, int b, int i, int j) {
+    static const int ca[6] = {0, 1, 2, 0, 0, 1}, cb[6] = {0, 1, 2, 1, 2, 2};
+    auto E = [&](int a, int b) {
       double s = 0;
       for (int m = 0; m < KQ; ++m)
         for (int q = 0; q < KQ; ++q) s += Tb::D[a][m][i] * Tb::MQ[m][q] * Tb::D[b][q][j];
       return s;
     };
-    static const int ca[6] = {0, 1, 2, 0, 0, 1}, cb[6] = {0, 1, 2, 1, 2, 2};
+    return ca[c] == cb[c] ? E(ca[c], cb[c]) : E(ca[c], cb[c]) + E(cb[c], ca[c]);
+  }
+  // round to TF32 (10 mantissa bits, nearest, ties away)
+  static float tf32_round(double v) {
+    float f = float(v);
+    uint32_t bits;
+    std::memcpy(&bits, &f, 4);
+    bits = (bits + 0x1000u) & 0xFFFFE000u;
+    std::memcpy(&f, &bits, 4);
+    return f;
+  }
+
+  template <int P>
+  void build_tc_tables() {
+    using Sh = CGTcShape<P>;
     std::vector<float> B(size_t(Sh::NPAD) * Sh::KPAD, 0.0f);
     for (int c = 0; c < 6; ++c)
       for (int i = 0; i < Sh::K; ++i)
-        for (int j = 0; j < Sh::K; ++j) {
-          double v = E(ca[c], cb[c], i, j);
-          if (ca[c] != cb[c]) v += E(cb[c], ca[c], i, j);
-          // round to TF32 (10 mantissa bits, nearest, ties away)
-          float f = float(v);
-          uint32_t bits;
-          std::memcpy(&bits, &f, 4);
-          bits = (bits + 0x1000u) & 0xFFFFE000u;
-          std::memcpy(&f, &bits, 4);
-          B[size_t(c * Sh::K + i) * Sh::KPAD + j] = f;
-        }
+        for (int j = 0; j < Sh::K; ++j) B[size_t(c * Sh::K + i) * Sh::KPAD + j] = tf32_round(stiffness_S<P>(c, i, j));
     d_btc.upload(B);
     int dev = 0, sms = 0, occ = 0;
     SFEM_CUDA(cudaGetDevice(&dev));
@@ -399,6 +405,46 @@ class CGOperator final : public Operator {
         d_constrained.p);
   }
 
+  // TF32 tensor-core cube kernel (variant 8, FP32 operators with cube tables):
+  // B rows p NP + n = (S_c)_i. for c = p CPP + n / K, i = n % K
+  DevBuf<float> d_bcube;
+  int cube_tc_grid = 0;
+  size_t cube_tc_smem = 0;
+  template <int P, int NB, int KP>
+  void setup_cube_tc() {
+    using Sh = CubeTcShape<P>;
+    std::vector<float> B(size_t(Sh::NBROWS) * Sh::KPAD, 0.0f);
+    for (int p = 0; p < Sh::PASSES; ++p)
+      for (int n = 0; n < Sh::CPP * Sh::K; ++n)
+        for (int j = 0; j < Sh::K; ++j)
+          B[size_t(p * Sh::NP + n) * Sh::KPAD + j] = tf32_round(stiffness_S<P>(p * Sh::CPP + n / Sh::K, n % Sh::K, j));
+    d_bcube.upload(B);
+    auto kern = cg_cube_tc_kernel<P, NB, KP>;
+    int dev = 0, sms = 0, occ = 0;
+    SFEM_CUDA(cudaGetDevice(&dev));
+    SFEM_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+    // more CTAs per SM than the tensor memory holds would wait in tcgen05.alloc
+    // for another CTA to finish: pad the shared memory until they cannot fit
+    size_t smem = Sh::smem_bytes(NB, KP);
+    for (;;) {
+      SFEM_REQUIRE(smem <= 227 * 1024, FEM_ERR_CUDA, "CG tensor-core cube kernel: no shared-memory size fits");
+      SFEM_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)));
+      SFEM_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, kern, 384, smem));
+      if (occ <= Sh::MAX_CTAS) break;
+      smem += 4096;
+    }
+    SFEM_REQUIRE(occ > 0, FEM_ERR_CUDA, "CG tensor-core cube kernel does not fit on an SM");
+    cube_tc_smem = smem;
+    cube_tc_grid = int(std::min<int64_t>(n_blocks, int64_t(sms) * occ));
+  }
+  template <int P, int NB, int KP>
+  void launch_cube_tc(const T* x, T* d, int sched, cudaStream_t s) {
+    cg_cube_tc_kernel<P, NB, KP><<<unsigned(cube_tc_grid), 384, cube_tc_smem, s>>>(
+        n_blocks, d_tmapv.p, d_bdof.p, d_ritem[sched].p, d_cslot8[sched].p, reinterpret_cast<const float*>(d_geo.p),
+        d_bcube.p, reinterpret_cast<const float*>(x), reinterpret_cast<float*>(d), d_constrained.n, d_constrained.p,
+        d_status.p);
+  }
+
   void build_hex_tables(const Mesh& mesh, const CGDofs& dofs, const std::vector<T>& geo) {
     if (n_cells == 0 || n_cells % 6 != 0 || int64_t(mesh.cell_hex.size()) != n_cells) return;
     const int64_t nh = n_cells / 6;
@@ -502,6 +548,13 @@ class CGOperator final : public Operator {
         case 2: setup_cube<2, 729, 11>(); break;
         case 3: setup_cube<3, 2197, 21>(); break;
       }
+      if (std::is_same<T, float>::value) {
+        switch (cfg.degree) {
+          case 1: setup_cube_tc<1, 125, 5>(); break;
+          case 2: setup_cube_tc<2, 729, 11>(); break;
+          case 3: setup_cube_tc<3, 2197, 21>(); break;
+        }
+      }
     }
     if (hex_H) {
       switch (cfg.degree) {
@@ -544,6 +597,20 @@ class CGOperator final : public Operator {
     // every SM two cubes (or two CTAs of hexes), where the coarser forms
     // leave SMs idle
     int v = cfg.kernel_variant;
+    if (v == 8) {
+      // TF32 tensor cores per cube; per cell (variant 4) without whole cubes
+      SFEM_REQUIRE(d_btc.p != nullptr, FEM_ERR_ARG, "CG kernel variant 8 (TF32 tensor cores) needs an FP32 operator");
+      if (cube_NB && cube_tc_grid) {
+        switch (cfg.degree) {
+          case 1: launch_cube_tc<1, 125, 5>(x, d, 0, s); break;
+          case 2: launch_cube_tc<2, 729, 11>(x, d, 0, s); break;
+          case 3: launch_cube_tc<3, 2197, 21>(x, d, 0, s); break;
+        }
+        SFEM_CUDA(cudaGetLastError());
+        return;
+      }
+      v = 4;
+    }
     if (v == 4) {
       SFEM_REQUIRE(d_btc.p != nullptr, FEM_ERR_ARG, "CG kernel variant 4 (TF32 tensor cores) needs an FP32 operator");
       launch_tc_cell(x, d, s);

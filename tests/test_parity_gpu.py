@@ -236,21 +236,24 @@ def test_autotuner_picks_a_variant_and_caches_it(cuda, tmp_path):
         sf.set_autotune_cache(None)
 
 
+@pytest.mark.parametrize("variant,shape", [(4, (6, 5, 7)), (8, (8, 8, 8)), (8, (8, 4, 12)), (8, (6, 5, 7))])
 @pytest.mark.parametrize("p", [1, 2, 3])
-def test_cg_tf32_tensor_core_variant(cuda, p):
-    """FP32 CG operator on the TF32 tensor cores (variant 4): the cell operator
-    as one [128 cells x K] x [K x 6K] tcgen05 product per tile.  TF32 keeps 10
-    mantissa bits: rel l2 <= 3e-3 against the FP64 oracle."""
-    mesh = sf.Mesh((6, 5, 7), jitter=0.1, seed=3)
+def test_cg_tf32_tensor_core_variant(cuda, p, variant, shape):
+    """FP32 CG operator on the TF32 tensor cores: per cell (variant 4, one
+    [128 cells x K] x [K x 6K] tcgen05 product per tile) and per cube (variant
+    8, three tiles of 128 tets per 4x4x4-hex cube with the cube kernel's gather
+    and reduction; on a mesh without whole cubes it runs as variant 4).  TF32
+    keeps 10 mantissa bits: rel l2 <= 3e-3 against the FP64 oracle."""
+    mesh = sf.Mesh(shape, jitter=0.1, seed=3)
     op = sf.Operator(mesh, p, "cg", "fp32")
-    op.set_kernel_variant(4)
+    op.set_kernel_variant(variant)
     x = seeded_src(op.m(), 1)
     y = run_product(op, x)
     assert op.status() == 0
     ref = orc.for_mesh(mesh, p, orc.CG).vmult(oracle_input(op, x))
     assert rel_l2(y, ref) <= 3e-3
     with pytest.raises(sf.FemError):
-        sf.Operator(mesh, p, "cg", "fp64").set_kernel_variant(4)
+        sf.Operator(mesh, p, "cg", "fp64").set_kernel_variant(variant)
 
 
 @pytest.mark.parametrize("variant", [1, 2, 3, 4, 5])
