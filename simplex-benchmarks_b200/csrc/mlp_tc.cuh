@@ -155,6 +155,22 @@ __global__ void __launch_bounds__(tc::THREADS, 2) mlp_tc_kernel(int64_t n, const
   for (int64_t tile = int64_t(blockIdx.x) * GROUPS + grp; tile < n_tiles; tile += int64_t(gridDim.x) * GROUPS) {
     const int64_t c = tile * TILE + t;
     const bool live = c < n;
+    if (MODE == 0) {
+      // the next tile's DoF-index rows (20 x 512 B) and features (128 x 40 B)
+      // into L2, one 128-byte line per thread, while this tile runs
+      const int64_t c1 = (tile + int64_t(gridDim.x) * GROUPS) * TILE;
+      if (c1 < n) {
+        const void* line = nullptr;
+        if (t < 4 * D::NR) {
+          const int64_t e = c1 + 32 * (t & 3);
+          if (e < n) line = dofs + (t >> 2) * n + e;
+        } else if (t < 4 * D::NR + 40) {
+          const int64_t e = c1 * 10 + 32 * (t - 4 * D::NR);
+          if (e < n * 10) line = feat + e;
+        }
+        if (line) asm volatile("prefetch.global.L2 [%0];" ::"l"(line));
+      }
+    }
     // ---- input row
     float x[K1];
     float scale = 0.0f;
