@@ -106,14 +106,51 @@ __device__ __forceinline__ void face_cf(const T (&G)[6], int f, T (&cf)[3]) {
   }
 }
 
-// coalesced copy of `rows` rows of n contiguous values into padded rows
+// coalesced copy of `rows` rows of N contiguous values into padded rows.  A
+// full block from a 16-byte aligned source takes 16-byte loads, all issued
+// before the first shared-memory store (N / (16 / sizeof(T)) per thread in
+// flight); other blocks copy value by value.
 template <int N, int S, int BS, typename T>
 __device__ __forceinline__ void stage_in(T* __restrict__ sm, const T* __restrict__ g, int rows) {
+  constexpr int V = 16 / int(sizeof(T));  // values per 16-byte load
+  if constexpr (N % V == 0) {
+    if (rows == BS && (reinterpret_cast<uintptr_t>(g) & 15u) == 0) {
+      constexpr int PER = N / V;  // 16-byte loads per thread
+      uint4 w[PER];
+#pragma unroll
+      for (int k = 0; k < PER; ++k) w[k] = __ldg(reinterpret_cast<const uint4*>(g) + k * BS + threadIdx.x);
+#pragma unroll
+      for (int k = 0; k < PER; ++k) {
+        const T* v = reinterpret_cast<const T*>(&w[k]);
+        const int e0 = (k * BS + threadIdx.x) * V;
+#pragma unroll
+        for (int q = 0; q < V; ++q) sm[((e0 + q) / N) * S + ((e0 + q) % N)] = v[q];
+      }
+      return;
+    }
+  }
   const int total = rows * N;
   for (int e = threadIdx.x; e < total; e += BS) sm[(e / N) * S + (e % N)] = __ldg(g + e);
 }
+// the reverse copy; full blocks to a 16-byte aligned destination take 16-byte stores
 template <int N, int S, int BS, typename T>
 __device__ __forceinline__ void stage_out(T* __restrict__ g, const T* __restrict__ sm, int rows) {
+  constexpr int V = 16 / int(sizeof(T));
+  if constexpr (N % V == 0) {
+    if (rows == BS && (reinterpret_cast<uintptr_t>(g) & 15u) == 0) {
+      constexpr int PER = N / V;
+#pragma unroll
+      for (int k = 0; k < PER; ++k) {
+        const int e0 = (k * BS + threadIdx.x) * V;
+        uint4 w;
+        T* v = reinterpret_cast<T*>(&w);
+#pragma unroll
+        for (int q = 0; q < V; ++q) v[q] = sm[((e0 + q) / N) * S + ((e0 + q) % N)];
+        reinterpret_cast<uint4*>(g)[k * BS + threadIdx.x] = w;
+      }
+      return;
+    }
+  }
   const int total = rows * N;
   for (int e = threadIdx.x; e < total; e += BS) g[e] = sm[(e / N) * S + (e % N)];
 }
