@@ -36,7 +36,7 @@ METRIC = "vmult DoF/s (FP64 vs mixed); Poisson solve time to 1e-8 (MG vs learned
 WORKLOAD = "DG SIPG Poisson vmult, P3 on 32^3 x 6 Kuhn tets (196,608 cells, 3,932,160 DoFs), jitter 0.1h"
 # dram__bytes_read.sum + dram__bytes_write.sum of one dg_apply_kernel<3,1,false,64,double>
 # launch on this workload (ncu --set full capture, 89.25 MB read + 14.0 MB written)
-APPLY_TRAFFIC_BYTES = 103.3e6
+APPLY_TRAFFIC_BYTES = 107.9e6
 
 
 def parse():
