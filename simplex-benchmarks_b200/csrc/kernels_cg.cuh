@@ -214,7 +214,7 @@ __device__ __forceinline__ void cube_reduce(int t, const int32_t* __restrict__ b
 // frees the prefetch registers but takes 6 x 384 values of shared memory, which
 // the L1 cache loses: measured on B200 it is faster for P3 FP32 (130 against
 // 136 us on 64^3) and P1 FP64 (155 against 177 us on 128^3), slower for P2
-// FP64 (421 against 396 us) and P3 FP64, even for P2 FP32.
+// FP64 (421 against 396 us) and P3 FP64, and no faster for P2 FP32.
 // Shared memory: ((6 x 384) + 2 NB + 384 KP + NZ) values, NZ = 16 zero slots
 // for 8-byte values (bank pairs), 32 for 4-byte values.
 template <int P, typename T>
