@@ -158,17 +158,20 @@ int fem_op_vmult(fem_op* op, void* dst, const void* src, void* stream);
  * copy-out of vector i-1 overlap.  Pageable host memory works, with copies
  * that do not overlap. */
 int fem_op_vmult_host(fem_op* op, int32_t n, void* const* dst_host, const void* const* src_host, void* stream);
-/* Same product as fem_op_vmult for FEM_DG / FEM_HELMHOLTZ operators, for
- * callers that must not allocate device memory at the call (their memory
- * pool owns the device, or cudaMalloc's implicit synchronisation and
- * unbounded latency are not allowed there).  No counterpart in the
- * reference.  The call allocates nothing: its scratch is a 16 MiB static
- * device array inside this library (held on every GPU that loads it until
- * exit); operators needing more scratch are rejected with FEM_ERR_ARG (DG P3
- * FP64: up to 87,381 cells).  All calls share that array, so calls that
- * overlap on the GPU race; order them on one stream.  The first call on a
- * device looks up the array's device address; make it before any stream
- * capture. */
+/* Same product as fem_op_vmult for FEM_DG / FEM_HELMHOLTZ operators, with
+ * the face-trace scratch taken from a 16 MiB static device array inside this
+ * library instead of the operator's own buffer.  No counterpart in the
+ * reference.  The call allocates nothing (nor does fem_op_vmult at the call;
+ * fem_op_create allocates the operator's tables and its own scratch once).
+ * It serves callers that cannot call cudaMalloc where they set up per-apply
+ * working memory (a framework's memory pool owns the device): every apply
+ * through it shares the one library-owned array.  The array is held on every
+ * GPU that loads the library, until exit, whether or not the call is used.
+ * Operators needing more scratch are rejected with FEM_ERR_ARG (DG P3 FP64:
+ * up to 87,381 cells).  All calls share the array, so calls that overlap on
+ * the GPU race; order them on one stream.  Each call outside stream capture
+ * looks up the array's device address; a call under capture reuses the last
+ * one, so make one call on the device before capturing. */
 int fem_op_vmult_static_scratch(fem_op* op, void* dst, const void* src, void* stream);
 /* Operator::Tvmult (CG/cells_batched/application.cc:1193-1197): the operator is symmetric. */
 int fem_op_Tvmult(fem_op* op, void* dst, const void* src, void* stream);

@@ -25,10 +25,23 @@ const char* last_error();
 
 #ifdef __CUDACC__
 #include <cuda_runtime.h>
+
+#include <atomic>
 #define SFEM_CUDA(call)                                                                   \
   do {                                                                                    \
     cudaError_t e_ = (call);                                                              \
     if (e_ != cudaSuccess)                                                                \
       throw ::sfem::Error(FEM_ERR_CUDA, std::string(#call) + ": " + cudaGetErrorString(e_)); \
   } while (0)
+
+namespace sfem {
+// Per-device one-time set-up (kernel attributes are set per device): returns
+// true the first time it is called with `mask` while device `dev` is current.
+// Bit d of the mask stands for device d; ordinals of 64 and above are refused.
+inline bool first_use_on_device(std::atomic<uint64_t>& mask, int dev) {
+  if (dev < 0 || dev >= 64) throw Error(FEM_ERR_INTERNAL, "device ordinal out of range (0..63)");
+  const uint64_t bit = uint64_t(1) << dev;
+  return (mask.fetch_or(bit) & bit) == 0;
+}
+}  // namespace sfem
 #endif

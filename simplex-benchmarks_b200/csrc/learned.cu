@@ -32,14 +32,12 @@ __global__ void gather_rows(int n, int width, const int32_t* __restrict__ perm, 
 template <int MODE, typename T>
 void launch_tc(int64_t n, const int32_t* dofs, const float* feat, const float* winv, const __nv_bfloat16* wb,
                const T* r, T* z, float* zout, int* status, cudaStream_t s) {
-  static bool configured = false;
+  static std::atomic<uint64_t> configured{0};
   auto kern = mlp_tc_kernel<MODE, T>;
-  if (!configured) {
-    SFEM_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, tc::SMEM_BYTES));
-    configured = true;
-  }
   int dev = 0, sms = 0;
   SFEM_CUDA(cudaGetDevice(&dev));
+  if (first_use_on_device(configured, dev))
+    SFEM_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, tc::SMEM_BYTES));
   SFEM_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
   const int64_t tiles = (n + tc::TILE - 1) / tc::TILE;
   const int64_t groups = (tiles + tc::GROUPS - 1) / tc::GROUPS;
@@ -154,12 +152,12 @@ void LearnedSmoother::apply(const Operator& op, const void* r, void* z, cudaStre
 }
 
 double LearnedSmoother::gradient(const float* X, const float* Y, int n, float* grad, cudaStream_t s) {
-  static bool configured = false;
+  static std::atomic<uint64_t> configured{0};
   const int smem = 2 * NP * int(sizeof(float));
-  if (!configured) {
+  int dev = 0;
+  SFEM_CUDA(cudaGetDevice(&dev));
+  if (first_use_on_device(configured, dev))
     SFEM_CUDA(cudaFuncSetAttribute(mlp_grad_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
-    configured = true;
-  }
   SFEM_CUDA(cudaMemsetAsync(grad, 0, sizeof(float) * NP, s));
   SFEM_CUDA(cudaMemsetAsync(loss_.p, 0, sizeof(float), s));
   const int grid = std::min((n + 127) / 128, 148 * 2);

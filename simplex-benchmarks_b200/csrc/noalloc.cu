@@ -1,14 +1,19 @@
 // DG / Helmholtz vmult whose scratch lives in a fixed, file-scope device array.
 //
-// Why: fem_op_vmult uses a scratch buffer (the published face normal
-// derivatives) that fem_op_create obtains with cudaMalloc.  Some callers must
-// not allocate device memory: an application whose memory pool (a framework's
-// caching allocator, a pre-reserved arena) already owns the whole device, or a
-// latency-bound loop where cudaMalloc/cudaFree, which may synchronise the
-// device and take unbounded time, are not allowed.  fem_op_vmult_static_scratch
-// gives them the same product with the scratch taken from g_static_scratch
-// below, a static device array that exists on every GPU that loads this
-// library, from module load until process exit.
+// What the call provides: it allocates no device memory, and it does not use
+// the operator's own scratch buffer (the published face normal derivatives,
+// which fem_op_create allocates once with the operator's other tables).  The
+// scratch comes instead from g_static_scratch below, a static device array
+// that exists on every GPU that loads this library, from module load until
+// process exit, whether or not this call is ever made (16 MiB per GPU).
+//
+// Who needs it: callers that cannot call cudaMalloc where they set up their
+// per-apply working memory - an application whose memory pool (a framework's
+// caching allocator, a pre-reserved arena) owns the rest of the device, or one
+// that must not add a device allocation per concurrent apply.  fem_op_vmult
+// allocates nothing at the call either; the difference is that every apply
+// through this entry point shares one library-owned buffer instead of the
+// operator's.  Creating the operator still allocates its tables.
 //
 // Limits and rules:
 //   - at most kStaticScratchBytes (16 MiB) of scratch: DG P3 FP64 up to 87,381
@@ -18,9 +23,11 @@
 //     to start at zero;
 //   - calls whose kernels overlap on the GPU (other streams, other threads)
 //     race on the array and give wrong results: order them on one stream;
-//   - on each device, the first call looks up the array's device address
-//     (cudaGetSymbolAddress, with that device current) and caches it; make
-//     that first call before any stream capture.
+//   - the array's device address is looked up (cudaGetSymbolAddress, with the
+//     device current) on every call made outside stream capture, so it stays
+//     right after a device reset; a call made while `stream` is capturing uses
+//     the address found by the last uncaptured call on that device, so make one
+//     call on each device before capturing.
 #include <cuda_runtime.h>
 
 #include <mutex>
@@ -41,19 +48,27 @@ void* g_scratch_ptr[kMaxDevices] = {};
 
 // Device address of g_static_scratch on the current device.  In host code the
 // symbol only names a host-side shadow; its device address must be looked up.
-void* static_scratch_address() {
+// Outside stream capture the lookup is repeated (it is cheap), so a context
+// that was reset and re-created never gets a stale address; under capture the
+// last looked-up address of the device is used.
+void* static_scratch_address(cudaStream_t stream) {
   int dev = -1;
   SFEM_CUDA(cudaGetDevice(&dev));
   SFEM_REQUIRE(dev >= 0 && dev < kMaxDevices, FEM_ERR_INTERNAL, "device ordinal out of range");
+  cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
+  SFEM_CUDA(cudaStreamIsCapturing(stream, &cap));
   std::lock_guard<std::mutex> lock(g_scratch_mu);
-  if (!g_scratch_ptr[dev]) {
-    void* p = nullptr;
-    const cudaError_t e = cudaGetSymbolAddress(&p, g_static_scratch);
-    if (e != cudaSuccess || p == nullptr)
-      throw Error(FEM_ERR_CUDA, std::string("cudaGetSymbolAddress(static scratch): ") + cudaGetErrorString(e));
-    g_scratch_ptr[dev] = p;
+  if (cap != cudaStreamCaptureStatusNone) {
+    SFEM_REQUIRE(g_scratch_ptr[dev] != nullptr, FEM_ERR_STATE,
+                 "fem_op_vmult_static_scratch: make one call on this device before stream capture");
+    return g_scratch_ptr[dev];
   }
-  return g_scratch_ptr[dev];
+  void* p = nullptr;
+  const cudaError_t e = cudaGetSymbolAddress(&p, g_static_scratch);
+  if (e != cudaSuccess || p == nullptr)
+    throw Error(FEM_ERR_CUDA, std::string("cudaGetSymbolAddress(static scratch): ") + cudaGetErrorString(e));
+  g_scratch_ptr[dev] = p;
+  return p;
 }
 
 }  // namespace
@@ -72,7 +87,8 @@ extern "C" int fem_op_vmult_static_scratch(fem_op* op, void* dst, const void* sr
                  "fem_op_vmult_static_scratch: operator needs " + std::to_string(need) +
                      " bytes of scratch, more than the static maximum of " +
                      std::to_string(sfem::kStaticScratchBytes) + " bytes");
-    void* scratch = sfem::static_scratch_address();
-    op->op->vmult_with_scratch(dst, src, scratch, sfem::kStaticScratchBytes, static_cast<cudaStream_t>(stream));
+    const cudaStream_t s = static_cast<cudaStream_t>(stream);
+    void* scratch = sfem::static_scratch_address(s);
+    op->op->vmult_with_scratch(dst, src, scratch, sfem::kStaticScratchBytes, s);
   });
 }

@@ -862,13 +862,11 @@ class DGOperator final : public Operator {
   }
 
   template <class K>
-  static void opt_in_smem(K kernel, size_t bytes, int& configured) {
+  static void opt_in_smem(K kernel, size_t bytes, std::atomic<uint64_t>& configured) {
     int dev = 0;
     SFEM_CUDA(cudaGetDevice(&dev));
-    if (!(configured & (1 << dev))) {
+    if (first_use_on_device(configured, dev))
       SFEM_CUDA(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, int(bytes)));
-      configured |= 1 << dev;
-    }
   }
 
   template <int P, int NC, bool MASS, int BS, int MINB = (BS == 64 ? 6 : 1), bool ALIAS = false>
@@ -878,7 +876,7 @@ class DGOperator final : public Operator {
     const DGBatch<T> b = make_batch(probs, n, BS, n_blocks);
     const size_t sm_trace = size_t(BS) * (S::US + S::QS) * sizeof(T);
     const size_t sm_apply = size_t(BS) * ((ALIAS ? 1 : 2) * S::US + S::QS) * sizeof(T);
-    static int conf_t = 0, conf_a = 0;
+    static std::atomic<uint64_t> conf_t{0}, conf_a{0};
     auto apply = dg_apply_kernel<P, NC, MASS, BS, T, MINB, ALIAS>;
     opt_in_smem(dg_trace_kernel<P, NC, BS, T>, sm_trace, conf_t);
     opt_in_smem(apply, sm_apply, conf_a);
@@ -893,7 +891,7 @@ class DGOperator final : public Operator {
     const DGBatch<T> b = make_batch(probs, n, D::CELLS, n_blocks);
     const size_t sm_trace = size_t(D::TRACE_ELEMS) * sizeof(T);
     const size_t sm_apply = size_t(D::APPLY_ELEMS) * sizeof(T);
-    static int conf_t = 0, conf_a = 0;
+    static std::atomic<uint64_t> conf_t{0}, conf_a{0};
     opt_in_smem(dg3_trace_kernel<P, NC, T>, sm_trace, conf_t);
     opt_in_smem(dg3_apply_kernel<P, NC, MASS, T>, sm_apply, conf_a);
     if (what != 2) dg3_trace_kernel<P, NC, T><<<unsigned(n_blocks), D::THREADS, sm_trace, s>>>(b, n_blocks);

@@ -17,6 +17,7 @@ _HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(_HERE, "libsimplexfem.so")
 
 FEM_OK = 0
+FEM_ERR_ARG, FEM_ERR_CUDA, FEM_ERR_STATE, FEM_ERR_INTERNAL = 1, 2, 3, 7
 FEM_CG, FEM_DG, FEM_HELMHOLTZ = 0, 1, 2
 FEM_FP64, FEM_FP32 = 0, 1
 FEM_PENALTY_REFERENCE, FEM_PENALTY_SQUARE = 0, 1

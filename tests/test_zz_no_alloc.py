@@ -1,9 +1,9 @@
-"""fem_op_vmult_static_scratch: the vmult for callers that cannot allocate.
+"""fem_op_vmult_static_scratch: the vmult whose scratch is a static array.
 
-Some callers may not allocate device memory where they apply the operator:
-their framework's memory pool already owns the device, or cudaMalloc's
-implicit synchronisation is not allowed on their hot path.  This entry point
-takes its scratch from a 16 MiB static device array inside the library.  The
+Some callers cannot call cudaMalloc where they set up per-apply working
+memory: their framework's memory pool already owns the device.  This entry
+point allocates nothing and takes its face-trace scratch from a 16 MiB static
+device array inside the library instead of the operator's own buffer.  The
 test calls it through the C ABI twice in a row (the second call finds the
 first call's leftovers in the shared array) and checks both results against
 fem_op_vmult, with the FP64 tolerance of the other parity tests.  It lives in
@@ -50,9 +50,10 @@ def test_static_scratch_rejects_oversized_and_cg(cuda):
     src = big.initialize_dof_vector()
     dst = big.initialize_dof_vector()
     stream = torch.cuda.current_stream()
-    assert _call(big, dst, src, stream) == 1
+    assert _call(big, dst, src, stream) == sf.FEM_ERR_ARG
     assert b"static maximum" in sf.lib().fem_last_error_string()
     cg = sf.Operator(sf.Mesh(3), 2, "cg", "fp64")
     v = cg.initialize_dof_vector()
     w = cg.initialize_dof_vector()
-    assert _call(cg, w, v, stream) == 1
+    assert _call(cg, w, v, stream) == sf.FEM_ERR_ARG
+    assert b"only DG and Helmholtz" in sf.lib().fem_last_error_string()
