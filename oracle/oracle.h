@@ -73,6 +73,17 @@ int oracle_cell_matrix(oracle_ctx* ctx, int64_t c, double* mat);
 int64_t oracle_check_cg_numbering(oracle_ctx* ctx, const double* lo, const double* hi);
 /* reference basis value / gradient (for known-answer tests) */
 int oracle_basis(int32_t degree, const double* xi, double* values, double* grads);
+/* The benchmark mesh, restated independently of the product (mesh.c): Kuhn
+ * tets of an n[0] x n[1] x n[2] hex box in Morton hex order, vertices
+ * jittered from an MT19937-64 stream.  Caller-allocated outputs:
+ * x [(n0+1)(n1+1)(n2+1)][3], cells/nb/nbf [6 n0 n1 n2][4].  Returns 0 on success. */
+int oracle_kuhn_mesh(const int32_t n[3], const double lo[3], const double hi[3], double jitter, uint64_t seed,
+                     double* x, int32_t* cells, int32_t* nb, int8_t* nbf);
+/* First-touch continuous P_degree numbering and Dirichlet mask of a mesh with
+ * sorted cell vertices.  Returns n_dofs (negative on error); with cell_dofs ==
+ * NULL only counts.  cell_dofs [n_cells][k], constrained [n_dofs]. */
+int64_t oracle_cg_numbering(int64_t n_vertices, int64_t n_cells, const int32_t* cells, const int32_t* nb,
+                            int32_t degree, int32_t* cell_dofs, uint8_t* constrained);
 /* quadrature sizes actually used */
 int oracle_quadrature_sizes(const oracle_ctx* ctx, int32_t* n_cell_points, int32_t* n_face_points);
 

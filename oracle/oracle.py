@@ -47,6 +47,12 @@ def lib():
         L.oracle_n_dofs.restype = C.c_int64
         L.oracle_n_dofs.argtypes = [C.c_void_p]
         L.oracle_quadrature_sizes.argtypes = [C.c_void_p, C.POINTER(C.c_int32), C.POINTER(C.c_int32)]
+        L.oracle_kuhn_mesh.restype = C.c_int
+        L.oracle_kuhn_mesh.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_double, C.c_uint64, C.c_void_p,
+                                       C.c_void_p, C.c_void_p, C.c_void_p]
+        L.oracle_cg_numbering.restype = C.c_int64
+        L.oracle_cg_numbering.argtypes = [C.c_int64, C.c_int64, C.c_void_p, C.c_void_p, C.c_int32, C.c_void_p,
+                                          C.c_void_p]
         _lib = L
     return _lib
 
@@ -123,8 +129,59 @@ def basis(degree, xi):
     return v, g
 
 
+class KuhnMesh:
+    """The benchmark mesh made by the oracle's own generator (mesh.c), with
+    the accessors of the product's Mesh (vertices, cells, neighbors, cg_dofs),
+    so the CPU checker and baseline never need the product library."""
+
+    def __init__(self, n, lo=(0.0, 0.0, 0.0), hi=(1.0, 1.0, 1.0), jitter=0.0, seed=0):
+        if isinstance(n, int):
+            n = (n, n, n)
+        self.n = tuple(int(v) for v in n)
+        nv = (self.n[0] + 1) * (self.n[1] + 1) * (self.n[2] + 1)
+        self.n_vertices = nv
+        self.n_cells = 6 * self.n[0] * self.n[1] * self.n[2]
+        self._x = np.empty((nv, 3), np.float64)
+        self._cells = np.empty((self.n_cells, 4), np.int32)
+        self._nb = np.empty((self.n_cells, 4), np.int32)
+        self._nbf = np.empty((self.n_cells, 4), np.int8)
+        nn = np.array(self.n, np.int32)
+        lo_, hi_ = np.array(lo, np.float64), np.array(hi, np.float64)
+        rc = lib().oracle_kuhn_mesh(nn.ctypes.data, lo_.ctypes.data, hi_.ctypes.data, float(jitter), int(seed),
+                                    self._x.ctypes.data, self._cells.ctypes.data, self._nb.ctypes.data,
+                                    self._nbf.ctypes.data)
+        if rc != 0:
+            raise RuntimeError(f"oracle_kuhn_mesh failed: {rc}")
+        self.n_boundary_faces = int((self._nb < 0).sum())
+        self.n_interior_faces = (4 * self.n_cells - self.n_boundary_faces) // 2
+        self._dofs = {}
+
+    def vertices(self):
+        return self._x
+
+    def cells(self):
+        return self._cells
+
+    def neighbors(self):
+        return self._nb, self._nbf
+
+    def cg_dofs(self, degree):
+        if degree not in self._dofs:
+            n = lib().oracle_cg_numbering(self.n_vertices, self.n_cells, self._cells.ctypes.data,
+                                          self._nb.ctypes.data, degree, None, None)
+            if n < 0:
+                raise RuntimeError(f"oracle_cg_numbering failed: {n}")
+            k = (degree + 1) * (degree + 2) * (degree + 3) // 6
+            cd = np.empty((self.n_cells, k), np.int32)
+            cm = np.empty(n, np.uint8)
+            lib().oracle_cg_numbering(self.n_vertices, self.n_cells, self._cells.ctypes.data,
+                                      self._nb.ctypes.data, degree, cd.ctypes.data, cm.ctypes.data)
+            self._dofs[degree] = (cd, cm)
+        return self._dofs[degree]
+
+
 def for_mesh(mesh, degree, kind, **kw):
-    """Oracle on a simplexfem.Mesh (CG uses the mesh's own CG numbering)."""
+    """Oracle on a simplexfem.Mesh or a KuhnMesh (CG uses the mesh's own CG numbering)."""
     if kind == CG:
         cd, cm = mesh.cg_dofs(degree)
         return Oracle(mesh.vertices(), mesh.cells(), degree, CG, cell_dofs=cd, constrained=cm, **kw)
