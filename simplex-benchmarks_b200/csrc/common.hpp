@@ -27,6 +27,8 @@ const char* last_error();
 #include <cuda_runtime.h>
 
 #include <atomic>
+
+#include "../../include/simplex_fem.h"
 #define SFEM_CUDA(call)                                                                   \
   do {                                                                                    \
     cudaError_t e_ = (call);                                                              \

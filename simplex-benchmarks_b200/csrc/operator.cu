@@ -7,6 +7,7 @@
 #include "kernels_cg.cuh"
 #include "kernels_cg_tc.cuh"
 #include "kernels_dg.cuh"
+#include "kernels_dg2.cuh"
 #include "kernels_dg3.cuh"
 #include "autotune.hpp"
 #include "operator.hpp"
@@ -869,7 +870,7 @@ class DGOperator final : public Operator {
       SFEM_CUDA(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, int(bytes)));
   }
 
-  template <int P, int NC, bool MASS, int BS, int MINB = (BS == 64 ? 6 : 1), bool ALIAS = false>
+  template <int P, int NC, bool MASS, int BS, int MINB = (BS == 64 ? 6 : 1), bool ALIAS = false, bool YS = false>
   static void run_cell(const DGProblem<T>* probs, int n, cudaStream_t s, int what) {
     using S = DGShape<P, NC>;
     int64_t n_blocks = 0;
@@ -877,10 +878,27 @@ class DGOperator final : public Operator {
     const size_t sm_trace = size_t(BS) * (S::US + S::QS) * sizeof(T);
     const size_t sm_apply = size_t(BS) * ((ALIAS ? 1 : 2) * S::US + S::QS) * sizeof(T);
     static std::atomic<uint64_t> conf_t{0}, conf_a{0};
-    auto apply = dg_apply_kernel<P, NC, MASS, BS, T, MINB, ALIAS>;
+    auto apply = dg_apply_kernel<P, NC, MASS, BS, T, MINB, ALIAS, YS>;
     opt_in_smem(dg_trace_kernel<P, NC, BS, T>, sm_trace, conf_t);
     opt_in_smem(apply, sm_apply, conf_a);
     if (what != 2) dg_trace_kernel<P, NC, BS, T><<<unsigned(n_blocks), BS, sm_trace, s>>>(b, n_blocks);
+    if (what != 1) apply<<<unsigned(n_blocks), BS, sm_apply, s>>>(b, n_blocks);
+  }
+
+  // phase-split scalar kernels (kernels_dg2.cuh): cross-block trace + apply
+  template <int P, bool MASS, int BS, int MINB, bool YS = false>
+  static void run_split(const DGProblem<T>* probs, int n, cudaStream_t s, int what) {
+    using S = DG2Shape<P, YS>;
+    int64_t n_blocks = 0;
+    const DGBatch<T> b = make_batch(probs, n, BS, n_blocks);
+    const size_t sm_trace = size_t(BS) * S::US * sizeof(T);
+    const size_t sm_apply = size_t(BS) * S::ELEMS * sizeof(T);
+    static std::atomic<uint64_t> conf_t{0}, conf_a{0};
+    auto trace = dg_trace_cross_kernel<P, BS, T>;
+    auto apply = dg_apply2_kernel<P, MASS, BS, T, MINB, YS>;
+    opt_in_smem(trace, sm_trace, conf_t);
+    opt_in_smem(apply, sm_apply, conf_a);
+    if (what != 2) trace<<<unsigned(n_blocks), BS, sm_trace, s>>>(b, n_blocks);
     if (what != 1) apply<<<unsigned(n_blocks), BS, sm_apply, s>>>(b, n_blocks);
   }
 
@@ -918,8 +936,25 @@ class DGOperator final : public Operator {
       // problems), registers capped for 8 CTAs per SM
       if (NC == 1) run_cell<P, NC, MASS, 64, 8, (NC == 1)>(probs, n, s, what);
       else run_cell<P, NC, MASS, 64, 8, false>(probs, n, s, what);
+    } else if (variant == 6) {
+      // 64 cells per CTA, 6 CTAs per SM, results accumulated in shared memory
+      // while the faces run
+      run_cell<P, NC, MASS, 64, 6, false, true>(probs, n, s, what);
+    } else if (variant >= 7 && variant <= 10) {
+      // phase-split scalar kernels: 7 / 8 results in registers, 64 cells x 5
+      // CTAs or 32 cells x 10 CTAs per SM; 9 / 10 results in shared memory,
+      // 64 cells x 4 CTAs or 32 cells x 8 CTAs; multi-component problems take
+      // the 128-cell form
+      if constexpr (NC == 1) {
+        if (variant == 7) run_split<P, MASS, 64, 5>(probs, n, s, what);
+        else if (variant == 8) run_split<P, MASS, 32, 10>(probs, n, s, what);
+        else if (variant == 9) run_split<P, MASS, 64, 4, true>(probs, n, s, what);
+        else run_split<P, MASS, 32, 8, true>(probs, n, s, what);
+      } else {
+        run_cell<P, NC, MASS, 128>(probs, n, s, what);
+      }
     } else {
-      throw Error(FEM_ERR_ARG, "DG: kernel variant must be 0..5");
+      throw Error(FEM_ERR_ARG, "DG: kernel variant must be 0..10");
     }
     SFEM_CUDA(cudaGetLastError());
   }

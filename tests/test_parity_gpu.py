@@ -256,11 +256,14 @@ def test_cg_tf32_tensor_core_variant(cuda, p, variant, shape):
         sf.Operator(mesh, p, "cg", "fp64").set_kernel_variant(variant)
 
 
-@pytest.mark.parametrize("variant", [1, 2, 3, 4, 5])
+@pytest.mark.parametrize("variant", [1, 2, 3, 4, 5, 6, 7, 8, 9, 10])
 @pytest.mark.parametrize("kind", ["dg", "helmholtz"])
 @pytest.mark.parametrize("p", [1, 2, 3])
 def test_dg_kernel_variants(cuda, p, kind, variant):
-    """Every DG / Helmholtz kernel shape (the autotuner's candidates) against the oracle, FP64."""
+    """Every DG / Helmholtz kernel shape (the autotuner's candidates) against
+    the oracle, FP64.  On 360 cells most faces of the phase-split forms (7-10)
+    cross a block boundary, so both neighbour paths (shared memory and the
+    published cross-block traces) run."""
     mesh = sf.Mesh((5, 4, 3), jitter=0.1, seed=2)
     op = sf.Operator(mesh, p, kind, "fp64")
     op.set_kernel_variant(variant)
@@ -268,6 +271,20 @@ def test_dg_kernel_variants(cuda, p, kind, variant):
     y = run_product(op, x)
     ref = orc.for_mesh(mesh, p, KIND[kind], n_components=op.n_components).vmult(x)
     assert rel_l2(y, ref) <= 1e-12
+
+
+@pytest.mark.parametrize("precision", ["fp64", "fp32"])
+def test_dg_kernel_variants_config2_full_size(cuda, precision):
+    """Every scalar DG kernel shape on the headline workload (DG P3, 32^3 x 6
+    tets, src U[-1,1] seed 1) against the oracle."""
+    mesh = sf.Mesh(32, jitter=0.1, seed=0)
+    op = sf.Operator(mesh, 3, "dg", precision)
+    x = seeded_src(op.m(), 1)
+    ref = orc.for_mesh(mesh, 3, orc.DG).vmult(oracle_input(op, x))
+    for v in range(1, 11):
+        op.set_kernel_variant(v)
+        err = rel_l2(run_product(op, x), ref)
+        assert err <= TOL[precision], (v, err)
 
 
 @pytest.mark.parametrize("kind", ["dg", "helmholtz"])
