@@ -51,8 +51,9 @@ def parse():
     ap.add_argument("--no-solve", action="store_true", help="skip the multigrid solve measurement")
     ap.add_argument("--no-extra", action="store_true", help="skip the CG (configs 1, 1L) and batch (config 4) lines")
     ap.add_argument("--no-learned", action="store_true", help="skip training and timing the learned smoother")
-    ap.add_argument("--case", choices=["cg-p2-64", "cg-p1-128", "cg-p2-128", "mlp-64"],
+    ap.add_argument("--case", choices=["cg-p2-64", "cg-p1-128", "cg-p2-128", "mlp-64", "dg-p3-32"],
                     help="run one small kernel workload (for profiling) instead of the benchmark")
+    ap.add_argument("--variant", type=int, default=0, help="kernel variant of --case dg-p3-32 (0: default)")
     return ap.parse_args()
 
 
@@ -588,16 +589,28 @@ def run_ours(args):
         dist.destroy_process_group()
 
 
-def run_case(name, reps=3):
+def run_case(name, reps=3, variant=0):
     """One small workload of a single kernel family, for profiling (ncu -k ...):
     cg-p2-64 / cg-p1-128 / cg-p2-128: CG vmults (default kernel variant, FP64 and
     FP32) on 64^3 or 128^3 x 6 tets, jitter 0.1h; mlp-64: eager V-cycles of the
     mixed multigrid with the learned finest-level smoother on CG P3 64^3
-    (untrained network: the kernels do the same work)."""
+    (untrained network: the kernels do the same work); dg-p3-32: FP64 vmults of
+    the headline DG P3 32^3 workload with kernel variant `variant`."""
     import torch
     import simplexfem as sf
     out = {"case": name}
-    if name.startswith("cg-"):
+    if name == "dg-p3-32":
+        mesh = sf.Mesh(N_HEX, jitter=JITTER, seed=0)
+        op = sf.Operator(mesh, DEGREE, "dg", "fp64")
+        if variant:
+            op.set_kernel_variant(variant)
+        x = torch.rand(op.m(), dtype=op.dtype, device="cuda")
+        y = op.initialize_dof_vector()
+        for _ in range(reps):
+            op.vmult(y, x)
+        torch.cuda.synchronize()
+        out.update({"m": op.m(), "variant": variant, "finite": bool(torch.isfinite(y).all())})
+    elif name.startswith("cg-"):
         p, n = int(name[4]), int(name.split("-")[2])
         mesh = sf.Mesh(n, jitter=JITTER, seed=0)
         for prec in ("fp64", "fp32"):
@@ -629,7 +642,7 @@ def run_case(name, reps=3):
 def main():
     args = parse()
     if args.case:
-        run_case(args.case)
+        run_case(args.case, variant=args.variant)
         return
     if args.impl == "reference":
         run_reference(args)

@@ -1000,7 +1000,7 @@ class DGBatchImpl final : public Batch {
   }
   int variant() const override { return cfg.kernel_variant; }
   void set_variant(int v) override {
-    SFEM_REQUIRE(v >= 0 && v <= 5, FEM_ERR_ARG, "batch: kernel variant must be 0..5");
+    SFEM_REQUIRE(v >= 0 && v <= 10, FEM_ERR_ARG, "batch: kernel variant must be 0..10");
     cfg.kernel_variant = v;
   }
   TuneResult tune(int reps, bool use_cache) override {
