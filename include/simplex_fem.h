@@ -198,6 +198,40 @@ int fem_op_work(const fem_op* op, double* flops, double* bytes);
  * in the reference (its kernels have no bounded waits). */
 int fem_op_status(fem_op* op, int32_t* status);
 
+/* ---- domain decomposition (one rank per GPU) -----------------------------
+ * Replaces the reference's distributed triangulation with a z-order
+ * partition (parallel::fullydistributed::Triangulation,
+ * CG/cells_batched/application.cc:1773-1801) and the ghost handling of its
+ * MPI-distributed vectors inside MatrixFree::cell_loop / loop
+ * (update_ghost_values before, compress(add) after; DG/cells_batched/
+ * application.cc:1303-1316).  Part r of n_parts owns a contiguous range of
+ * the hierarchical cell order (cut at 4x4x4-hex cubes or hexes when possible).
+ * Its local vectors hold [owned entries | ghost entries]: CG DoFs (a DoF
+ * belongs to the part of the first cell touching it) or DG cell blocks (the
+ * ghosts are the face neighbours of the part's cells).  For each peer, the
+ * send list (local indices of owned entries the peer holds as ghosts) and the
+ * receive list (local indices of ghosts the peer owns) are in ascending
+ * global index, so they match entry by entry.  Before each vmult the caller
+ * copies send -> peer's recv (ghost update); after a CG vmult it adds the
+ * ghost entries back into their owners' entries along the same lists
+ * (compress) and may clear them.  The partition itself is host-only. */
+typedef struct fem_part fem_part;
+int fem_part_create(const fem_mesh* mesh, int32_t degree, int32_t kind, int32_t n_components, int32_t n_parts,
+                    int32_t part, fem_part** out);
+int fem_part_destroy(fem_part* part);
+int fem_part_sizes(const fem_part* part, int64_t* n_owned, int64_t* n_ghost, int64_t* n_global,
+                   int64_t* cell_begin, int64_t* cell_end, int32_t* n_peers);
+/* global vector index of every local entry, [n_owned + n_ghost] */
+int fem_part_global_index(const fem_part* part, int64_t* gidx);
+/* peer i (ascending rank): its rank and the lengths of its send / receive lists */
+int fem_part_peer(const fem_part* part, int32_t i, int32_t* rank, int64_t* n_send, int64_t* n_recv);
+int fem_part_halo(const fem_part* part, int32_t i, int64_t* send /* [n_send] */, int64_t* recv /* [n_recv] */);
+/* The part's local operator on its local vectors (m() = n_owned + n_ghost):
+ * the owned rows of dst are the global operator's rows once the ghosts of src
+ * are up to date (CG: after the compress); DG ghost rows hold no meaning.
+ * The partition may be destroyed afterwards. */
+int fem_op_create_part(const fem_part* part, int32_t precision, const fem_op_params* params, fem_op** out);
+
 /* ---- loads --------------------------------------------------------------
  * f(x) = sum_m amp[m] sin(k[m] . x)           (kind FEM_RHS_PLANE_WAVES)
  *      = sum_m amp[m] prod_d sin(k[m][d] x_d)  (kind FEM_RHS_SINE_PRODUCTS) */

@@ -105,12 +105,12 @@ int fem_mesh_cg_dofs(const fem_mesh* mesh, int32_t degree, int64_t* n_dofs, int3
   });
 }
 
-int fem_op_create(fem_mesh* mesh, int32_t degree, int32_t kind, int32_t precision, const fem_op_params* params,
-                  fem_op** out) {
-  return guarded([&] {
-    REQUIRE_PTR(mesh);
-    REQUIRE_PTR(out);
-    sfem::OpConfig cfg;
+}  // extern "C"
+
+namespace sfem {
+// fem_op_params -> OpConfig, with the checks of fem_op_create
+OpConfig op_config(int32_t degree, int32_t kind, int32_t precision, const fem_op_params* params) {
+    OpConfig cfg;
     cfg.degree = degree;
     cfg.kind = kind;
     cfg.precision = precision;
@@ -132,6 +132,18 @@ int fem_op_create(fem_mesh* mesh, int32_t degree, int32_t kind, int32_t precisio
       SFEM_REQUIRE(cfg.penalty == FEM_PENALTY_REFERENCE || cfg.penalty == FEM_PENALTY_SQUARE, FEM_ERR_ARG,
                    "penalty must be FEM_PENALTY_REFERENCE or FEM_PENALTY_SQUARE");
     }
+    return cfg;
+}
+}  // namespace sfem
+
+extern "C" {
+
+int fem_op_create(fem_mesh* mesh, int32_t degree, int32_t kind, int32_t precision, const fem_op_params* params,
+                  fem_op** out) {
+  return guarded([&] {
+    REQUIRE_PTR(mesh);
+    REQUIRE_PTR(out);
+    const sfem::OpConfig cfg = sfem::op_config(degree, kind, precision, params);
     auto o = std::make_unique<fem_op>();
     o->op = sfem::make_operator(mesh->mesh, cfg);
     *out = o.release();

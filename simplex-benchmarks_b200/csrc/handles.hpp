@@ -6,12 +6,16 @@
 #include "mesh.hpp"
 #include "mg.hpp"
 #include "operator.hpp"
+#include "partition.hpp"
 
 struct fem_mesh {
   sfem::Mesh mesh;
 };
 struct fem_op {
   std::unique_ptr<sfem::Operator> op;
+};
+struct fem_part {
+  sfem::Partition p;
 };
 struct fem_batch {
   std::unique_ptr<sfem::Batch> batch;
@@ -28,6 +32,8 @@ struct fem_cg {
 };
 
 namespace sfem {
+OpConfig op_config(int32_t degree, int32_t kind, int32_t precision, const fem_op_params* params);
+
 // Runs f, converting exceptions into a status code and the last-error string.
 template <class F>
 int guarded(F&& f) {

@@ -503,9 +503,15 @@ class CGOperator final : public Operator {
     hex_H = H;
   }
 
-  CGOperator(const Mesh& mesh, const OpConfig& c) {
+  CGOperator(const Mesh& mesh, const OpConfig& c) : CGOperator(mesh, build_cg_dofs(mesh, c.degree), nullptr, c) {}
+
+  // Operator on the cells of `mesh` with a given numbering: dofs.constrained
+  // masks the gather and scatter, `identity` (default: dofs.constrained)
+  // lists the rows that get dst = src.  A partition's local operator passes
+  // the global constraints of its owned and ghost DoFs and only the owned
+  // constrained DoFs as identity rows.
+  CGOperator(const Mesh& mesh, CGDofs dofs, const std::vector<uint8_t>* identity, const OpConfig& c) {
     cfg = c;
-    CGDofs dofs = build_cg_dofs(mesh, cfg.degree);
     K = dofs.K;
     n_cells = mesh.n_cells;
     m = dofs.n_dofs;
@@ -529,8 +535,10 @@ class CGOperator final : public Operator {
     }
     d_geo.upload(geo);
     std::vector<int32_t> cl;
+    const std::vector<uint8_t>& id_rows = identity ? *identity : constrained;
+    SFEM_REQUIRE(int64_t(id_rows.size()) == m, FEM_ERR_INTERNAL, "CG: identity mask size");
     for (int64_t i = 0; i < m; ++i)
-      if (constrained[i]) cl.push_back(int32_t(i));
+      if (id_rows[i]) cl.push_back(int32_t(i));
     d_constrained.upload(cl);
     build_hex_tables(mesh, dofs, geo);
     build_cube_tables(dofs);
@@ -739,7 +747,7 @@ class DGOperator final : public Operator {
         face_area_normal(mesh, cc, f, a, nrm);
         area[4 * cc + f] = a;
         inv_h[4 * cc + f] = 2.0 * a / absdet[cc];  // |grad lambda_f| = 1/h_f
-        surf += a * (mesh.nb[4 * cc + f] < 0 ? 1.0 : 0.5);
+        surf += a * (mesh.nb[4 * cc + f] == -1 ? 1.0 : 0.5);  // -2: interior, neighbour not local
       }
       tau[cc] = surf / (absdet[cc] / 6.0);
     }
@@ -765,7 +773,7 @@ class DGOperator final : public Operator {
     std::vector<int8_t> nbf(4 * size_t(n_cells));
     for (int64_t cc = 0; cc < n_cells; ++cc)
       for (int f = 0; f < 4; ++f) {
-        nb[size_t(f) * n_cells + cc] = mesh.nb[4 * cc + f];
+        nb[size_t(f) * n_cells + cc] = std::max(mesh.nb[4 * cc + f], -1);
         nbf[size_t(f) * n_cells + cc] = mesh.nbf[4 * cc + f] < 0 ? 0 : mesh.nbf[4 * cc + f];
       }
     d_nb.upload(nb);
@@ -1083,6 +1091,23 @@ std::unique_ptr<Operator> make_operator(const Mesh& mesh, const OpConfig& cfg) {
     throw Error(FEM_ERR_ARG, "operator: unknown kind");
   }
   op->mesh = &mesh;
+  return op;
+}
+
+std::unique_ptr<Operator> make_local_operator(std::shared_ptr<const Mesh> mesh, const CGDofs* dofs,
+                                              const std::vector<uint8_t>* identity, const OpConfig& cfg) {
+  SFEM_REQUIRE(cfg.degree >= 1 && cfg.degree <= 3, FEM_ERR_ARG, "operator: degree must be 1, 2 or 3");
+  SFEM_REQUIRE(cfg.precision == FEM_FP64 || cfg.precision == FEM_FP32, FEM_ERR_ARG, "operator: bad precision");
+  std::unique_ptr<Operator> op;
+  if (cfg.kind == FEM_CG) {
+    SFEM_REQUIRE(dofs && identity, FEM_ERR_INTERNAL, "CG local operator needs its numbering");
+    if (cfg.precision == FEM_FP64) op = std::make_unique<CGOperator<double>>(*mesh, *dofs, identity, cfg);
+    else op = std::make_unique<CGOperator<float>>(*mesh, *dofs, identity, cfg);
+  } else {
+    op = make_operator(*mesh, cfg);
+  }
+  op->mesh = mesh.get();
+  op->owned_mesh = std::move(mesh);
   return op;
 }
 

@@ -72,6 +72,7 @@ class Operator {
   std::shared_ptr<HostPipe> host_pipe;  // created by the first vmult_host
   OpConfig cfg;
   const Mesh* mesh = nullptr;  // the mesh the operator was built on (must outlive it)
+  std::shared_ptr<const Mesh> owned_mesh;  // set when the operator keeps its own (partition-local) mesh
   int K = 0;               // DoFs per cell and component
   int64_t n_cells = 0;
   int64_t m = 0;           // vector length
@@ -115,6 +116,11 @@ struct RhsDesc {
 double rhs_value(const RhsDesc& r, const double* x);
 
 std::unique_ptr<Operator> make_operator(const Mesh& mesh, const OpConfig& cfg);
+// Operator on a partition-local mesh it keeps alive: CG takes the given
+// numbering (dofs) and identity rows; DG / Helmholtz read nb == -2 as an
+// interior face whose neighbour is not in the local mesh.
+std::unique_ptr<Operator> make_local_operator(std::shared_ptr<const Mesh> mesh, const CGDofs* dofs,
+                                              const std::vector<uint8_t>* identity, const OpConfig& cfg);
 
 // Outcome of an autotuning run (autotune.hpp).
 struct TuneResult {

@@ -107,6 +107,15 @@ _PROTOS = [
     ("fem_op_vmult_host", C.c_int, [C.c_void_p, C.c_int32, C.c_void_p, C.c_void_p, C.c_void_p]),
     ("fem_op_work", C.c_int, [C.c_void_p, C.POINTER(C.c_double), C.POINTER(C.c_double)]),
     ("fem_op_status", C.c_int, [C.c_void_p, C.POINTER(C.c_int32)]),
+    ("fem_part_create", C.c_int, [C.c_void_p, C.c_int32, C.c_int32, C.c_int32, C.c_int32, C.c_int32,
+                                  C.POINTER(C.c_void_p)]),
+    ("fem_part_destroy", C.c_int, [C.c_void_p]),
+    ("fem_part_sizes", C.c_int, [C.c_void_p] + [C.POINTER(C.c_int64)] * 5 + [C.POINTER(C.c_int32)]),
+    ("fem_part_global_index", C.c_int, [C.c_void_p, C.c_void_p]),
+    ("fem_part_peer", C.c_int, [C.c_void_p, C.c_int32, C.POINTER(C.c_int32), C.POINTER(C.c_int64),
+                                C.POINTER(C.c_int64)]),
+    ("fem_part_halo", C.c_int, [C.c_void_p, C.c_int32, C.c_void_p, C.c_void_p]),
+    ("fem_op_create_part", C.c_int, [C.c_void_p, C.c_int32, C.POINTER(OpParams), C.POINTER(C.c_void_p)]),
     ("fem_op_rhs", C.c_int, [C.c_void_p, C.POINTER(RhsDesc), C.c_void_p, C.c_void_p]),
     ("fem_op_interpolate", C.c_int, [C.c_void_p, C.POINTER(RhsDesc), C.c_void_p, C.c_void_p]),
     ("fem_mg_params_default", C.c_int, [C.POINTER(MGParams)]),
@@ -243,7 +252,9 @@ class Operator:
     """Matrix-free operator (fem_op); the drop-in for the reference's Operator."""
 
     def __init__(self, mesh, degree, kind="cg", precision="fp64", mass=1e5, n_components=None,
-                 penalty=FEM_PENALTY_REFERENCE):
+                 penalty=FEM_PENALTY_REFERENCE, partition=None):
+        """partition: a Partition of `mesh`; the operator is then that part's
+        local operator on [owned | ghost] vectors (fem_op_create_part)."""
         self.mesh = mesh
         k = KINDS[kind] if isinstance(kind, str) else kind
         pr = PRECISIONS[precision] if isinstance(precision, str) else precision
@@ -252,7 +263,13 @@ class Operator:
         p.n_components = n_components or (3 if k == FEM_HELMHOLTZ else 1)
         p.penalty = penalty
         h = C.c_void_p()
-        check(lib().fem_op_create(mesh.handle, degree, k, pr, C.byref(p), C.byref(h)))
+        if partition is None:
+            check(lib().fem_op_create(mesh.handle, degree, k, pr, C.byref(p), C.byref(h)))
+        else:
+            if (partition.degree, partition.kind) != (degree, k):
+                raise FemError(FEM_ERR_ARG, "partition made for another degree or kind")
+            check(lib().fem_op_create_part(partition.handle, pr, C.byref(p), C.byref(h)))
+        self.partition = partition
         self.handle = h
         self.kind, self.precision, self.degree = k, pr, degree
         m = C.c_uint64()
@@ -352,6 +369,46 @@ class Operator:
     def __del__(self):
         if getattr(self, "handle", None) and _lib is not None:
             _lib.fem_op_destroy(self.handle)
+            self.handle = None
+
+
+class Partition:
+    """Part `part` of `n_parts` of a mesh for one rank (fem_part): contiguous
+    ranges of the hierarchical cell order; local vectors are [owned | ghost]
+    entries (CG DoFs, DG cell blocks) with per-peer send / receive lists."""
+
+    def __init__(self, mesh, degree, kind, n_parts, part, n_components=None):
+        k = KINDS[kind] if isinstance(kind, str) else kind
+        nc = n_components or (3 if k == FEM_HELMHOLTZ else 1)
+        h = C.c_void_p()
+        check(lib().fem_part_create(mesh.handle, degree, k, nc, n_parts, part, C.byref(h)))
+        self.handle = h
+        self.mesh, self.degree, self.kind, self.n_components = mesh, degree, k, nc
+        self.n_parts, self.part = n_parts, part
+        no, ng, ngl, cb, ce = (C.c_int64() for _ in range(5))
+        npeer = C.c_int32()
+        check(lib().fem_part_sizes(h, C.byref(no), C.byref(ng), C.byref(ngl), C.byref(cb), C.byref(ce),
+                                   C.byref(npeer)))
+        self.n_owned, self.n_ghost, self.n_global = no.value, ng.value, ngl.value
+        self.cell_range = (cb.value, ce.value)
+        self.global_index = np.empty(self.n_owned + self.n_ghost, np.int64)
+        check(lib().fem_part_global_index(h, self.global_index.ctypes.data))
+        self.peers = []  # (rank, send local indices, recv local indices)
+        for i in range(npeer.value):
+            r, ns, nr = C.c_int32(), C.c_int64(), C.c_int64()
+            check(lib().fem_part_peer(h, i, C.byref(r), C.byref(ns), C.byref(nr)))
+            snd = np.empty(ns.value, np.int64)
+            rcv = np.empty(nr.value, np.int64)
+            check(lib().fem_part_halo(h, i, snd.ctypes.data, rcv.ctypes.data))
+            self.peers.append((r.value, snd, rcv))
+
+    @property
+    def m(self):
+        return self.n_owned + self.n_ghost
+
+    def __del__(self):
+        if getattr(self, "handle", None) and _lib is not None:
+            _lib.fem_part_destroy(self.handle)
             self.handle = None
 
 
