@@ -125,8 +125,8 @@ OpConfig op_config(int32_t degree, int32_t kind, int32_t precision, const fem_op
       }
       cfg.penalty = params->penalty;
       cfg.kernel_variant = params->kernel_variant;
-      SFEM_REQUIRE(cfg.kernel_variant >= 0 && cfg.kernel_variant <= (kind == FEM_CG ? 8 : 10), FEM_ERR_ARG,
-                   "kernel_variant must be 0..8 (CG) or 0..10 (DG, Helmholtz)");
+      SFEM_REQUIRE(cfg.kernel_variant >= 0 && cfg.kernel_variant <= (kind == FEM_CG ? 8 : 12), FEM_ERR_ARG,
+                   "kernel_variant must be 0..8 (CG) or 0..12 (DG, Helmholtz)");
       SFEM_REQUIRE((cfg.kernel_variant != 4 && cfg.kernel_variant != 8) || kind != FEM_CG || precision == FEM_FP32,
                    FEM_ERR_ARG, "CG kernel_variant 4 and 8 (TF32 tensor cores) are for FP32 operators");
       SFEM_REQUIRE(cfg.penalty == FEM_PENALTY_REFERENCE || cfg.penalty == FEM_PENALTY_SQUARE, FEM_ERR_ARG,
@@ -259,8 +259,8 @@ int fem_op_vmult_host(fem_op* op, int32_t n, void* const* dst_host, const void* 
 int fem_op_set_kernel_variant(fem_op* op, int32_t variant) {
   return guarded([&] {
     REQUIRE_PTR(op);
-    SFEM_REQUIRE(variant >= 0 && variant <= (op->op->cfg.kind == FEM_CG ? 8 : 10), FEM_ERR_ARG,
-                 "kernel_variant must be 0..8 (CG) or 0..10 (DG, Helmholtz)");
+    SFEM_REQUIRE(variant >= 0 && variant <= (op->op->cfg.kind == FEM_CG ? 8 : 12), FEM_ERR_ARG,
+                 "kernel_variant must be 0..8 (CG) or 0..12 (DG, Helmholtz)");
     SFEM_REQUIRE((variant != 4 && variant != 8) || op->op->cfg.kind != FEM_CG || op->op->cfg.precision == FEM_FP32,
                  FEM_ERR_ARG, "CG kernel_variant 4 and 8 (TF32 tensor cores) are for FP32 operators");
     op->op->cfg.kernel_variant = variant;

@@ -90,6 +90,18 @@ struct DGShape {
   static constexpr int QS = padded(QN);
 };
 
+// asynchronous global -> shared copies of one element (LDGSTS)
+template <typename T>
+__device__ __forceinline__ void cp_async_elem(T* smem, const T* gmem) {
+  const unsigned s = static_cast<unsigned>(__cvta_generic_to_shared(smem));
+  if constexpr (sizeof(T) == 8)
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(s), "l"(gmem) : "memory");
+  else
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 4;\n" ::"r"(s), "l"(gmem) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_group 0;\n" ::: "memory"); }
+
 // J^-1 (2|F_f| n_f) for local face f
 template <typename T>
 __device__ __forceinline__ void face_cf(const T (&G)[6], int f, T (&cf)[3]) {
@@ -210,12 +222,16 @@ __global__ void __launch_bounds__(BS) dg_trace_kernel(const __grid_constant__ DG
 // YS: the results accumulate in the shared-memory row `ys` (stride 1) instead
 // of registers while the faces run, and come back to registers only for the
 // final transposed contraction (fewer live registers, no spills).
-template <int P, int NC, bool MASS, bool HAVE_NB, typename T, bool YS = false>
+// XS: `xs` points at this cell's staged cross-block neighbour data, one row
+// of XROW values per face slot (slot[f] < 0: not staged): the neighbour's
+// face values already in this cell's face-node order, then its traces.
+template <int P, int NC, bool MASS, bool HAVE_NB, typename T, bool YS = false, bool XS = false>
 __device__ __forceinline__ void dg_cell_component(const DGProblem<T>& pr, int64_t c0, int comp,
                                                   const T* us, const T* qs, const T* su, const T* sq, int nloc,
                                                   const T (&G)[6], const T (&sf)[4], T md,
                                                   const int32_t (&nb)[4], const int (&nbf)[4],
-                                                  T (&y)[gen::Ops<P>::K], T* ys = nullptr) {
+                                                  T (&y)[gen::Ops<P>::K], T* ys = nullptr,
+                                                  const T* xs = nullptr, const int (*slot)[4] = nullptr) {
   using O = gen::Ops<P>;
   using S = DGShape<P, NC>;
   constexpr int K = O::K, KQ = O::KQ, NF = O::NF, NFQ = O::NFQ;
@@ -246,7 +262,13 @@ __device__ __forceinline__ void dg_cell_component(const DGProblem<T>& pr, int64_
     const T* qm = qs + (f * NC + comp) * NFQ;
     T j[NF], avg[NFQ];
     if (nb[f] >= 0) {
-      if (HAVE_NB) {
+      if (XS && (*slot)[f] >= 0) {
+        const T* xn = xs + (*slot)[f] * (NF + NFQ);
+#pragma unroll
+        for (int i = 0; i < NF; ++i) j[i] = u[O::fn(f, i)] - xn[i];
+#pragma unroll
+        for (int m = 0; m < NFQ; ++m) avg[m] = T(0.25) * (qm[m] - xn[NF + m]);
+      } else if (HAVE_NB) {
         const int64_t lc = int64_t(nb[f]) - c0;
         const T* un;
         const T* qn;
@@ -381,6 +403,96 @@ __global__ void __launch_bounds__(BS, MINB) dg_apply_kernel(const __grid_constan
 #pragma unroll
         for (int i = 0; i < O::K; ++i) sy[t * S::US + comp * O::K + i] = y[i];
       }
+    }
+    __syncthreads();
+    stage_out<S::U, S::US, BS>(pr.dst + c0 * S::U, sy, nloc);
+  }
+}
+
+// Apply with the cross-block neighbour data prefetched (scalar problems).
+// Faces whose neighbour lies outside the CTA's BS cells read the neighbour's
+// face values and published traces from global memory, one dependent load
+// chain per face, which a thread-per-cell kernel at 2 warps per scheduler
+// cannot hide.  Here, while the CTA stages its own rows, every thread also
+// issues cp.async copies of its cross-block faces' neighbour data (face
+// values permuted into its own face-node order, then the traces) into
+// compact shared-memory rows: a CTA-wide prefix sum over the cross faces
+// gives the rows, up to XCAP of them; faces past XCAP (rare) keep the direct
+// global reads.  All copies are in flight together and land before the
+// compute starts.
+template <int P, int BS, int XCAP, typename T>
+__global__ void __launch_bounds__(BS, 1) dg_apply_xp_kernel(const __grid_constant__ DGBatch<T> batch,
+                                                            int64_t n_blocks) {
+  using O = gen::Ops<P>;
+  using S = DGShape<P, 1>;
+  constexpr int XROW = O::NF + O::NFQ;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  T* su = reinterpret_cast<T*>(smem_raw);  // [BS][US]  src rows
+  T* sq = su + BS * S::US;                 // [BS][QS]  published traces
+  T* sy = sq + BS * S::QS;                 // [BS][US]  results
+  T* sx = sy + BS * S::US;                 // [XCAP][XROW] cross-block neighbour rows
+  __shared__ int warp_tot[BS / 32];
+  for (int64_t blk = blockIdx.x; blk < n_blocks; blk += gridDim.x) {
+    const int pi = find_problem(batch, blk);
+    const DGProblem<T>& pr = batch.p[pi];
+    const int64_t c0 = (blk - batch.block_begin[pi]) * BS;
+    const int nloc = int(pr.n_cells - c0 < BS ? pr.n_cells - c0 : int64_t(BS));
+    const int t = threadIdx.x;
+    const int64_t n = pr.n_cells;
+    CellData<T> d;
+    int cross = 0;  // bit f: face f has its neighbour outside this CTA
+    if (t < nloc) {
+      load_cell<false>(pr, c0 + t, d);
+#pragma unroll
+      for (int f = 0; f < 4; ++f) {
+        const int64_t lc = int64_t(d.nb[f]) - c0;
+        if (d.nb[f] >= 0 && (lc < 0 || lc >= nloc)) cross |= 1 << f;
+      }
+    }
+    // CTA-wide exclusive prefix sum of the cross-face counts
+    const int cnt = __popc(cross);
+    const int lane = t & 31, warp = t >> 5;
+    int incl = cnt;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const int v = __shfl_up_sync(0xffffffffu, incl, o);
+      if (lane >= o) incl += v;
+    }
+    __syncthreads();  // the previous block is done with every shared buffer
+    if (lane == 31) warp_tot[warp] = incl;
+    stage_in<S::U, S::US, BS>(su, pr.src + c0 * S::U, nloc);
+    stage_in<S::QN, S::QS, BS>(sq, pr.Q + c0 * S::QN, nloc);
+    __syncthreads();
+    int base = incl - cnt;
+    for (int w = 0; w < warp; ++w) base += warp_tot[w];
+    int slot[4];
+#pragma unroll
+    for (int f = 0; f < 4; ++f) {
+      slot[f] = -1;
+      if (cross >> f & 1) {
+        if (base < XCAP) {
+          slot[f] = base;
+          T* dst = sx + base * XROW;
+          const int nf = d.nbf[f];
+          const T* un = pr.src + int64_t(d.nb[f]) * O::K;
+          const T* qn = pr.Q + (int64_t(d.nb[f]) * 4 + nf) * O::NFQ;
+#pragma unroll
+          for (int i = 0; i < O::NF; ++i) cp_async_elem(dst + i, un + O::fn_runtime(nf, i));
+#pragma unroll
+          for (int m = 0; m < O::NFQ; ++m) cp_async_elem(dst + O::NF + m, qn + m);
+        }
+        ++base;
+      }
+    }
+    cp_async_commit();
+    cp_async_wait_all();
+    __syncthreads();
+    if (t < nloc) {
+      T y[O::K];
+      dg_cell_component<P, 1, false, true, T, false, true>(pr, c0, 0, su + t * S::US, sq + t * S::QS, su, sq, nloc,
+                                                          d.G, d.sf, d.md, d.nb, d.nbf, y, nullptr, sx, &slot);
+#pragma unroll
+      for (int i = 0; i < O::K; ++i) sy[t * S::US + i] = y[i];
     }
     __syncthreads();
     stage_out<S::U, S::US, BS>(pr.dst + c0 * S::U, sy, nloc);

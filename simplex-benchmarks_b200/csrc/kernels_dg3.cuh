@@ -51,18 +51,6 @@ struct DG3 {
   static constexpr int TRACE_ELEMS = CELLS * US + 3 * KQ * CELLS + CELLS * QS;
 };
 
-// asynchronous global -> shared copies of one element (LDGSTS)
-template <typename T>
-__device__ __forceinline__ void cp_async_elem(T* smem, const T* gmem) {
-  const unsigned s = static_cast<unsigned>(__cvta_generic_to_shared(smem));
-  if constexpr (sizeof(T) == 8)
-    asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(s), "l"(gmem) : "memory");
-  else
-    asm volatile("cp.async.ca.shared.global [%0], [%1], 4;\n" ::"r"(s), "l"(gmem) : "memory");
-}
-__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
-__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_group 0;\n" ::: "memory"); }
-
 // cf_f[a] = (J^-1 2|F_f| n_f)_a from the symmetric metric G
 template <typename T>
 __device__ __forceinline__ T cf_comp(const T (&G)[6], int f, int a) {

@@ -893,6 +893,24 @@ class DGOperator final : public Operator {
     if (what != 1) apply<<<unsigned(n_blocks), BS, sm_apply, s>>>(b, n_blocks);
   }
 
+  // trace + apply with the cross-block neighbour data prefetched (scalar problems)
+  template <int P, int BS, int XCAP>
+  static void run_xp(const DGProblem<T>* probs, int n, cudaStream_t s, int what) {
+    using S = DGShape<P, 1>;
+    using O = gen::Ops<P>;
+    int64_t n_blocks = 0;
+    const DGBatch<T> b = make_batch(probs, n, BS, n_blocks);
+    const size_t sm_trace = size_t(BS) * (S::US + S::QS) * sizeof(T);
+    const size_t sm_apply = (size_t(BS) * (2 * S::US + S::QS) + size_t(XCAP) * (O::NF + O::NFQ)) * sizeof(T);
+    static std::atomic<uint64_t> conf_t{0}, conf_a{0};
+    auto trace = dg_trace_kernel<P, 1, BS, T>;
+    auto apply = dg_apply_xp_kernel<P, BS, XCAP, T>;
+    opt_in_smem(trace, sm_trace, conf_t);
+    opt_in_smem(apply, sm_apply, conf_a);
+    if (what != 2) trace<<<unsigned(n_blocks), BS, sm_trace, s>>>(b, n_blocks);
+    if (what != 1) apply<<<unsigned(n_blocks), BS, sm_apply, s>>>(b, n_blocks);
+  }
+
   // phase-split scalar kernels (kernels_dg2.cuh): cross-block trace + apply
   template <int P, bool MASS, int BS, int MINB, bool YS = false>
   static void run_split(const DGProblem<T>* probs, int n, cudaStream_t s, int what) {
@@ -961,8 +979,18 @@ class DGOperator final : public Operator {
       } else {
         run_cell<P, NC, MASS, 128>(probs, n, s, what);
       }
+    } else if (variant == 11 || variant == 12) {
+      // 128 cells per CTA (11) or 64 (12), cross-block neighbour data
+      // prefetched into shared memory; multi-component problems take the
+      // 128-cell form
+      if constexpr (NC == 1 && !MASS) {
+        if (variant == 11) run_xp<P, 128, 192>(probs, n, s, what);
+        else run_xp<P, 64, 128>(probs, n, s, what);
+      } else {
+        run_cell<P, NC, MASS, 128>(probs, n, s, what);
+      }
     } else {
-      throw Error(FEM_ERR_ARG, "DG: kernel variant must be 0..10");
+      throw Error(FEM_ERR_ARG, "DG: kernel variant must be 0..12");
     }
     SFEM_CUDA(cudaGetLastError());
   }
@@ -1008,7 +1036,7 @@ class DGBatchImpl final : public Batch {
   }
   int variant() const override { return cfg.kernel_variant; }
   void set_variant(int v) override {
-    SFEM_REQUIRE(v >= 0 && v <= 10, FEM_ERR_ARG, "batch: kernel variant must be 0..10");
+    SFEM_REQUIRE(v >= 0 && v <= 12, FEM_ERR_ARG, "batch: kernel variant must be 0..12");
     cfg.kernel_variant = v;
   }
   TuneResult tune(int reps, bool use_cache) override {
