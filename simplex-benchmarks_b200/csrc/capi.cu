@@ -108,6 +108,11 @@ int fem_mesh_cg_dofs(const fem_mesh* mesh, int32_t degree, int64_t* n_dofs, int3
 }  // extern "C"
 
 namespace sfem {
+bool valid_variant(int kind, int v) {
+  if (kind == FEM_CG) return v >= 0 && v <= 8;
+  return (v >= 0 && v <= 5) || v == 7 || v == 9 || v == 11;
+}
+
 // fem_op_params -> OpConfig, with the checks of fem_op_create
 OpConfig op_config(int32_t degree, int32_t kind, int32_t precision, const fem_op_params* params) {
     OpConfig cfg;
@@ -125,8 +130,8 @@ OpConfig op_config(int32_t degree, int32_t kind, int32_t precision, const fem_op
       }
       cfg.penalty = params->penalty;
       cfg.kernel_variant = params->kernel_variant;
-      SFEM_REQUIRE(cfg.kernel_variant >= 0 && cfg.kernel_variant <= (kind == FEM_CG ? 8 : 12), FEM_ERR_ARG,
-                   "kernel_variant must be 0..8 (CG) or 0..12 (DG, Helmholtz)");
+      SFEM_REQUIRE(valid_variant(kind, cfg.kernel_variant), FEM_ERR_ARG,
+                   "kernel_variant must be 0..8 (CG) or 0..5, 7, 9, 11 (DG, Helmholtz)");
       SFEM_REQUIRE((cfg.kernel_variant != 4 && cfg.kernel_variant != 8) || kind != FEM_CG || precision == FEM_FP32,
                    FEM_ERR_ARG, "CG kernel_variant 4 and 8 (TF32 tensor cores) are for FP32 operators");
       SFEM_REQUIRE(cfg.penalty == FEM_PENALTY_REFERENCE || cfg.penalty == FEM_PENALTY_SQUARE, FEM_ERR_ARG,
@@ -259,8 +264,8 @@ int fem_op_vmult_host(fem_op* op, int32_t n, void* const* dst_host, const void* 
 int fem_op_set_kernel_variant(fem_op* op, int32_t variant) {
   return guarded([&] {
     REQUIRE_PTR(op);
-    SFEM_REQUIRE(variant >= 0 && variant <= (op->op->cfg.kind == FEM_CG ? 8 : 12), FEM_ERR_ARG,
-                 "kernel_variant must be 0..8 (CG) or 0..12 (DG, Helmholtz)");
+    SFEM_REQUIRE(sfem::valid_variant(op->op->cfg.kind, variant), FEM_ERR_ARG,
+                 "kernel_variant must be 0..8 (CG) or 0..5, 7, 9, 11 (DG, Helmholtz)");
     SFEM_REQUIRE((variant != 4 && variant != 8) || op->op->cfg.kind != FEM_CG || op->op->cfg.precision == FEM_FP32,
                  FEM_ERR_ARG, "CG kernel_variant 4 and 8 (TF32 tensor cores) are for FP32 operators");
     op->op->cfg.kernel_variant = variant;

@@ -219,19 +219,16 @@ __global__ void __launch_bounds__(BS) dg_trace_kernel(const __grid_constant__ DG
 // staged rows of this cell (`us`, `qs`); HAVE_NB reads the neighbour traces
 // (from shared memory when the neighbour is in this CTA, rows su/sq),
 // otherwise they are zero (diagonal).
-// YS: the results accumulate in the shared-memory row `ys` (stride 1) instead
-// of registers while the faces run, and come back to registers only for the
-// final transposed contraction (fewer live registers, no spills).
 // XS: `xs` points at this cell's staged cross-block neighbour data, one row
 // of XROW values per face slot (slot[f] < 0: not staged): the neighbour's
 // face values already in this cell's face-node order, then its traces.
-template <int P, int NC, bool MASS, bool HAVE_NB, typename T, bool YS = false, bool XS = false>
+template <int P, int NC, bool MASS, bool HAVE_NB, typename T, bool XS = false>
 __device__ __forceinline__ void dg_cell_component(const DGProblem<T>& pr, int64_t c0, int comp,
                                                   const T* us, const T* qs, const T* su, const T* sq, int nloc,
                                                   const T (&G)[6], const T (&sf)[4], T md,
                                                   const int32_t (&nb)[4], const int (&nbf)[4],
-                                                  T (&y)[gen::Ops<P>::K], T* ys = nullptr,
-                                                  const T* xs = nullptr, const int (*slot)[4] = nullptr) {
+                                                  T (&y)[gen::Ops<P>::K], const T* xs = nullptr,
+                                                  const int (*slot)[4] = nullptr) {
   using O = gen::Ops<P>;
   using S = DGShape<P, NC>;
   constexpr int K = O::K, KQ = O::KQ, NF = O::NF, NFQ = O::NFQ;
@@ -250,10 +247,6 @@ __device__ __forceinline__ void dg_cell_component(const DGProblem<T>& pr, int64_
 #pragma unroll
     for (int i = 0; i < K; ++i) y[i] = T(0);
     if (MASS) O::massP(uu, md, y);
-    if (YS) {
-#pragma unroll
-      for (int i = 0; i < K; ++i) ys[i] = y[i];
-    }
   }
 #pragma unroll
   for (int f = 0; f < 4; ++f) {
@@ -304,13 +297,8 @@ __device__ __forceinline__ void dg_cell_component(const DGProblem<T>& pr, int64_
 #pragma unroll
     for (int m = 0; m < NFQ; ++m) avg[m] = -avg[m];
     O::facePQ(avg, t);
-    if (YS) {
 #pragma unroll
-      for (int i = 0; i < NF; ++i) ys[O::fn(f, i)] += t[i];
-    } else {
-#pragma unroll
-      for (int i = 0; i < NF; ++i) y[O::fn(f, i)] += t[i];
-    }
+    for (int i = 0; i < NF; ++i) y[O::fn(f, i)] += t[i];
     // gradient test: h_a += -1/4 cf_a MFQP j
     T r[NFQ];
     O::faceQP(j, r);
@@ -322,10 +310,6 @@ __device__ __forceinline__ void dg_cell_component(const DGProblem<T>& pr, int64_
       h[KQ + nq] += cf[1] * rm;
       h[2 * KQ + nq] += cf[2] * rm;
     }
-  }
-  if (YS) {
-#pragma unroll
-    for (int i = 0; i < K; ++i) y[i] = ys[i];
   }
   O::gradT(h, y);
 }
@@ -356,14 +340,12 @@ __device__ __forceinline__ void load_cell(const DGProblem<T>& pr, int64_t c, Cel
 // results stay in registers until every thread of the CTA is done reading the
 // staged src rows, then reuse those rows for the coalesced write-out, so the
 // CTA needs no separate result rows (less shared memory, more CTAs per SM).
-template <int P, int NC, bool MASS, int BS, typename T, int MINB = (BS == 64 ? 6 : 1), bool ALIAS = false,
-          bool YS = false>
+template <int P, int NC, bool MASS, int BS, typename T, int MINB = (BS == 64 ? 6 : 1), bool ALIAS = false>
 __global__ void __launch_bounds__(BS, MINB) dg_apply_kernel(const __grid_constant__ DGBatch<T> batch,
                                                             int64_t n_blocks) {
   using O = gen::Ops<P>;
   using S = DGShape<P, NC>;
   static_assert(!ALIAS || NC == 1, "result aliasing holds one component in registers");
-  static_assert(!(ALIAS && YS), "results accumulated in shared memory need their own rows");
   extern __shared__ __align__(16) unsigned char smem_raw[];
   T* su = reinterpret_cast<T*>(smem_raw);  // [BS][US]  src rows
   T* sq = su + BS * S::US;                 // [BS][QS]  published traces
@@ -397,9 +379,8 @@ __global__ void __launch_bounds__(BS, MINB) dg_apply_kernel(const __grid_constan
 #pragma unroll 1
       for (int comp = 0; comp < NC; ++comp) {
         T y[O::K];
-        dg_cell_component<P, NC, MASS, true, T, YS>(pr, c0, comp, su + t * S::US, sq + t * S::QS, su, sq, nloc,
-                                                    d.G, d.sf, d.md, d.nb, d.nbf, y,
-                                                    sy + t * S::US + comp * O::K);
+        dg_cell_component<P, NC, MASS, true>(pr, c0, comp, su + t * S::US, sq + t * S::QS, su, sq, nloc, d.G,
+                                             d.sf, d.md, d.nb, d.nbf, y);
 #pragma unroll
         for (int i = 0; i < O::K; ++i) sy[t * S::US + comp * O::K + i] = y[i];
       }
@@ -489,8 +470,8 @@ __global__ void __launch_bounds__(BS, 1) dg_apply_xp_kernel(const __grid_constan
     __syncthreads();
     if (t < nloc) {
       T y[O::K];
-      dg_cell_component<P, 1, false, true, T, false, true>(pr, c0, 0, su + t * S::US, sq + t * S::QS, su, sq, nloc,
-                                                          d.G, d.sf, d.md, d.nb, d.nbf, y, nullptr, sx, &slot);
+      dg_cell_component<P, 1, false, true, T, true>(pr, c0, 0, su + t * S::US, sq + t * S::QS, su, sq, nloc, d.G,
+                                                   d.sf, d.md, d.nb, d.nbf, y, sx, &slot);
 #pragma unroll
       for (int i = 0; i < O::K; ++i) sy[t * S::US + i] = y[i];
     }

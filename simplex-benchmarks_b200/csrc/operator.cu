@@ -878,7 +878,7 @@ class DGOperator final : public Operator {
       SFEM_CUDA(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, int(bytes)));
   }
 
-  template <int P, int NC, bool MASS, int BS, int MINB = (BS == 64 ? 6 : 1), bool ALIAS = false, bool YS = false>
+  template <int P, int NC, bool MASS, int BS, int MINB = (BS == 64 ? 6 : 1), bool ALIAS = false>
   static void run_cell(const DGProblem<T>* probs, int n, cudaStream_t s, int what) {
     using S = DGShape<P, NC>;
     int64_t n_blocks = 0;
@@ -886,7 +886,7 @@ class DGOperator final : public Operator {
     const size_t sm_trace = size_t(BS) * (S::US + S::QS) * sizeof(T);
     const size_t sm_apply = size_t(BS) * ((ALIAS ? 1 : 2) * S::US + S::QS) * sizeof(T);
     static std::atomic<uint64_t> conf_t{0}, conf_a{0};
-    auto apply = dg_apply_kernel<P, NC, MASS, BS, T, MINB, ALIAS, YS>;
+    auto apply = dg_apply_kernel<P, NC, MASS, BS, T, MINB, ALIAS>;
     opt_in_smem(dg_trace_kernel<P, NC, BS, T>, sm_trace, conf_t);
     opt_in_smem(apply, sm_apply, conf_a);
     if (what != 2) dg_trace_kernel<P, NC, BS, T><<<unsigned(n_blocks), BS, sm_trace, s>>>(b, n_blocks);
@@ -962,35 +962,23 @@ class DGOperator final : public Operator {
       // problems), registers capped for 8 CTAs per SM
       if (NC == 1) run_cell<P, NC, MASS, 64, 8, (NC == 1)>(probs, n, s, what);
       else run_cell<P, NC, MASS, 64, 8, false>(probs, n, s, what);
-    } else if (variant == 6) {
-      // 64 cells per CTA, 6 CTAs per SM, results accumulated in shared memory
-      // while the faces run
-      run_cell<P, NC, MASS, 64, 6, false, true>(probs, n, s, what);
-    } else if (variant >= 7 && variant <= 10) {
-      // phase-split scalar kernels: 7 / 8 results in registers, 64 cells x 5
-      // CTAs or 32 cells x 10 CTAs per SM; 9 / 10 results in shared memory,
-      // 64 cells x 4 CTAs or 32 cells x 8 CTAs; multi-component problems take
-      // the 128-cell form
+    } else if (variant == 7 || variant == 9) {
+      // phase-split scalar kernels (kernels_dg2.cuh): 7 results in registers,
+      // 64 cells x 5 CTAs per SM; 9 results in shared memory, 64 cells x 4
+      // CTAs (no spills); multi-component problems take the 128-cell form
       if constexpr (NC == 1) {
         if (variant == 7) run_split<P, MASS, 64, 5>(probs, n, s, what);
-        else if (variant == 8) run_split<P, MASS, 32, 10>(probs, n, s, what);
-        else if (variant == 9) run_split<P, MASS, 64, 4, true>(probs, n, s, what);
-        else run_split<P, MASS, 32, 8, true>(probs, n, s, what);
+        else run_split<P, MASS, 64, 4, true>(probs, n, s, what);
       } else {
         run_cell<P, NC, MASS, 128>(probs, n, s, what);
       }
-    } else if (variant == 11 || variant == 12) {
-      // 128 cells per CTA (11) or 64 (12), cross-block neighbour data
-      // prefetched into shared memory; multi-component problems take the
-      // 128-cell form
-      if constexpr (NC == 1 && !MASS) {
-        if (variant == 11) run_xp<P, 128, 192>(probs, n, s, what);
-        else run_xp<P, 64, 128>(probs, n, s, what);
-      } else {
-        run_cell<P, NC, MASS, 128>(probs, n, s, what);
-      }
+    } else if (variant == 11) {
+      // 128 cells per CTA with the cross-block neighbour data prefetched into
+      // shared memory; multi-component and mass problems take the 128-cell form
+      if constexpr (NC == 1 && !MASS) run_xp<P, 128, 192>(probs, n, s, what);
+      else run_cell<P, NC, MASS, 128>(probs, n, s, what);
     } else {
-      throw Error(FEM_ERR_ARG, "DG: kernel variant must be 0..12");
+      throw Error(FEM_ERR_ARG, "DG: kernel variant must be 0..5, 7, 9 or 11");
     }
     SFEM_CUDA(cudaGetLastError());
   }
@@ -1036,7 +1024,8 @@ class DGBatchImpl final : public Batch {
   }
   int variant() const override { return cfg.kernel_variant; }
   void set_variant(int v) override {
-    SFEM_REQUIRE(v >= 0 && v <= 12, FEM_ERR_ARG, "batch: kernel variant must be 0..12");
+    SFEM_REQUIRE(v >= 0 && v <= 11 && v != 6 && v != 8 && v != 10, FEM_ERR_ARG,
+                 "batch: kernel variant must be 0..5, 7, 9 or 11");
     cfg.kernel_variant = v;
   }
   TuneResult tune(int reps, bool use_cache) override {

@@ -256,13 +256,13 @@ def test_cg_tf32_tensor_core_variant(cuda, p, variant, shape):
         sf.Operator(mesh, p, "cg", "fp64").set_kernel_variant(variant)
 
 
-@pytest.mark.parametrize("variant", [1, 2, 3, 4, 5, 6, 7, 8, 9, 10, 11, 12])
+@pytest.mark.parametrize("variant", [1, 2, 3, 4, 5, 7, 9, 11])
 @pytest.mark.parametrize("kind", ["dg", "helmholtz"])
 @pytest.mark.parametrize("p", [1, 2, 3])
 def test_dg_kernel_variants(cuda, p, kind, variant):
     """Every DG / Helmholtz kernel shape (the autotuner's candidates) against
-    the oracle, FP64.  On 360 cells most faces of the phase-split forms (7-10)
-    and of the prefetching forms (11, 12) cross a block boundary, so both
+    the oracle, FP64.  On 360 cells most faces of the phase-split forms (7, 9)
+    and of the prefetching form (11) cross a block boundary, so both
     neighbour paths (shared memory and the published cross-block traces) run."""
     mesh = sf.Mesh((5, 4, 3), jitter=0.1, seed=2)
     op = sf.Operator(mesh, p, kind, "fp64")
@@ -281,7 +281,7 @@ def test_dg_kernel_variants_config2_full_size(cuda, precision):
     op = sf.Operator(mesh, 3, "dg", precision)
     x = seeded_src(op.m(), 1)
     ref = orc.for_mesh(mesh, 3, orc.DG).vmult(oracle_input(op, x))
-    for v in range(1, 13):
+    for v in (1, 2, 3, 4, 5, 7, 9, 11):
         op.set_kernel_variant(v)
         err = rel_l2(run_product(op, x), ref)
         assert err <= TOL[precision], (v, err)
