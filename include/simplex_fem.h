@@ -108,6 +108,21 @@ int fem_version(int32_t* major, int32_t* minor);
 
 /* ---- mesh -------------------------------------------------------------- */
 int fem_mesh_create(const fem_mesh_desc* desc, fem_mesh** out);
+/* Unstructured tetrahedral mesh from arrays (the reference reads one with
+ * GridIn::read_vtk and reorders it with SparsityTools::reorder_hierarchical,
+ * CG/cells_batched/application.cc:1696-1757).  Cells may list their vertices
+ * in any order (stored sorted by vertex id; orientation does not matter).
+ * reorder = 1: cells in Morton order of their centroids (the hierarchical
+ * order the kernels' locality relies on); 0: input order.  Degenerate cells,
+ * vertex ids out of range and faces shared by more than two cells are
+ * FEM_ERR_ARG.  Such meshes take the per-cell kernels; multigrid needs a
+ * Kuhn box (fem_mesh_create). */
+int fem_mesh_create_from_arrays(int64_t n_vertices, const double* xyz /* [n_vertices][3] */, int64_t n_cells,
+                                const int32_t* cell_vertices /* [n_cells][4] */, int32_t reorder, fem_mesh** out);
+/* The same from a legacy ASCII VTK unstructured grid of tetrahedra (VTK cell type 10). */
+int fem_mesh_read_vtk(const char* path, int32_t reorder, fem_mesh** out);
+/* input index of every cell of a mesh from arrays (identity for Kuhn meshes) */
+int fem_mesh_copy_input_cells(const fem_mesh* mesh, int64_t* input_cell /* [n_cells] */);
 int fem_mesh_destroy(fem_mesh* mesh);
 int fem_mesh_sizes(const fem_mesh* mesh, int64_t* n_vertices, int64_t* n_cells,
                    int64_t* n_interior_faces, int64_t* n_boundary_faces);

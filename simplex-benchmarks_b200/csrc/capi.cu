@@ -54,6 +54,37 @@ int fem_mesh_create(const fem_mesh_desc* desc, fem_mesh** out) {
   });
 }
 
+int fem_mesh_create_from_arrays(int64_t n_vertices, const double* xyz, int64_t n_cells, const int32_t* cell_vertices,
+                                int32_t reorder, fem_mesh** out) {
+  return guarded([&] {
+    REQUIRE_PTR(xyz);
+    REQUIRE_PTR(cell_vertices);
+    REQUIRE_PTR(out);
+    auto m = std::make_unique<fem_mesh>();
+    m->mesh = sfem::build_mesh_from_arrays(n_vertices, xyz, n_cells, cell_vertices, reorder);
+    *out = m.release();
+  });
+}
+
+int fem_mesh_read_vtk(const char* path, int32_t reorder, fem_mesh** out) {
+  return guarded([&] {
+    REQUIRE_PTR(path);
+    REQUIRE_PTR(out);
+    auto m = std::make_unique<fem_mesh>();
+    m->mesh = sfem::read_vtk_mesh(path, reorder);
+    *out = m.release();
+  });
+}
+
+int fem_mesh_copy_input_cells(const fem_mesh* mesh, int64_t* input_cell) {
+  return guarded([&] {
+    REQUIRE_PTR(mesh);
+    REQUIRE_PTR(input_cell);
+    const sfem::Mesh& m = mesh->mesh;
+    for (int64_t c = 0; c < m.n_cells; ++c) input_cell[c] = m.input_cell.empty() ? c : m.input_cell[c];
+  });
+}
+
 int fem_mesh_destroy(fem_mesh* mesh) {
   return guarded([&] { delete mesh; });
 }

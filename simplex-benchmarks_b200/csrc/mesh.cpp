@@ -3,7 +3,9 @@
 
 #include <algorithm>
 #include <cmath>
+#include <fstream>
 #include <random>
+#include <string>
 
 #include "common.hpp"
 #include "ref_tables.h"
@@ -117,6 +119,12 @@ Mesh build_kuhn_mesh(const MeshDescription& d) {
     }
   }
 
+  build_face_adjacency(m);
+  m.structured = true;
+  return m;
+}
+
+void build_face_adjacency(Mesh& m) {
   // face adjacency: a face is found from its lowest vertex; the other two
   // vertices identify it among the faces incident to that vertex.
   Incidence inc = vertex_cells(m);
@@ -137,7 +145,8 @@ Mesh build_kuhn_mesh(const MeshDescription& d) {
         if (fv[0] != a) continue;
         bool matched = false;
         for (auto& p : local) {
-          if (p.b == fv[1] && p.c2 == fv[2] && p.cell >= 0) {
+          if (p.b == fv[1] && p.c2 == fv[2]) {
+            SFEM_REQUIRE(p.cell >= 0, FEM_ERR_ARG, "mesh: a face is shared by more than two cells");
             m.nb[4 * int64_t(cc) + f] = p.cell;
             m.nbf[4 * int64_t(cc) + f] = p.f;
             m.nb[4 * int64_t(p.cell) + p.f] = cc;
@@ -151,6 +160,7 @@ Mesh build_kuhn_mesh(const MeshDescription& d) {
       }
     }
   }
+  m.n_boundary_faces = m.n_interior_faces = 0;
   for (int64_t i = 0; i < 4 * m.n_cells; ++i) {
     if (m.nb[i] < 0)
       m.n_boundary_faces++;
@@ -158,7 +168,125 @@ Mesh build_kuhn_mesh(const MeshDescription& d) {
       m.n_interior_faces++;
   }
   m.n_interior_faces /= 2;
+}
+
+Mesh build_mesh_from_arrays(int64_t n_vertices, const double* x, int64_t n_cells, const int32_t* cells,
+                            int reorder) {
+  SFEM_REQUIRE(n_vertices >= 4 && n_cells >= 1, FEM_ERR_ARG, "mesh: need at least 4 vertices and 1 cell");
+  SFEM_REQUIRE(n_vertices < (int64_t(1) << 31) && n_cells < (int64_t(1) << 31), FEM_ERR_ARG,
+               "mesh: too many vertices or cells for int32 ids");
+  SFEM_REQUIRE(reorder == 0 || reorder == 1, FEM_ERR_ARG, "mesh: reorder must be 0 (input order) or 1 (Morton)");
+  Mesh m;
+  m.desc.n[0] = m.desc.n[1] = m.desc.n[2] = 0;
+  m.n_vertices = n_vertices;
+  m.n_cells = n_cells;
+  m.x.assign(x, x + 3 * n_vertices);
+  // hierarchical cell order: Morton order of the cell centroids on a 2^21 grid
+  // over the bounding box (the role of SparsityTools::reorder_hierarchical
+  // and DoFRenumbering::matrix_free_data_locality in the reference,
+  // CG/cells_batched/application.cc:1696-1757,1828)
+  std::vector<int64_t> order(n_cells);
+  for (int64_t c = 0; c < n_cells; ++c) order[c] = c;
+  for (int64_t c = 0; c < n_cells; ++c)
+    for (int v = 0; v < 4; ++v)
+      SFEM_REQUIRE(cells[4 * c + v] >= 0 && cells[4 * c + v] < n_vertices, FEM_ERR_ARG,
+                   "mesh: cell " + std::to_string(c) + " names a vertex out of range");
+  if (reorder == 1) {
+    double lo[3] = {1e300, 1e300, 1e300}, hi[3] = {-1e300, -1e300, -1e300};
+    for (int64_t v = 0; v < n_vertices; ++v)
+      for (int a = 0; a < 3; ++a) {
+        lo[a] = std::min(lo[a], x[3 * v + a]);
+        hi[a] = std::max(hi[a], x[3 * v + a]);
+      }
+    std::vector<uint64_t> key(n_cells);
+    for (int64_t c = 0; c < n_cells; ++c) {
+      uint64_t q[3];
+      for (int a = 0; a < 3; ++a) {
+        double s = 0;
+        for (int v = 0; v < 4; ++v) s += x[3 * int64_t(cells[4 * c + v]) + a];
+        const double t = (s / 4 - lo[a]) / std::max(hi[a] - lo[a], 1e-300);
+        q[a] = uint64_t(std::min(std::max(t, 0.0), 1.0) * double((1 << 21) - 1));
+      }
+      key[c] = morton3(q[0], q[1], q[2]);
+    }
+    std::stable_sort(order.begin(), order.end(), [&](int64_t a, int64_t b) { return key[a] < key[b]; });
+  }
+  m.cell_vertices.resize(4 * n_cells);
+  m.cell_hex.resize(n_cells);
+  m.input_cell.resize(n_cells);
+  for (int64_t c = 0; c < n_cells; ++c) {
+    int32_t vs[4];
+    for (int v = 0; v < 4; ++v) vs[v] = cells[4 * order[c] + v];
+    std::sort(vs, vs + 4);
+    SFEM_REQUIRE(vs[0] != vs[1] && vs[1] != vs[2] && vs[2] != vs[3], FEM_ERR_ARG,
+                 "mesh: cell " + std::to_string(order[c]) + " repeats a vertex");
+    for (int v = 0; v < 4; ++v) m.cell_vertices[4 * c + v] = vs[v];
+    m.cell_hex[c] = int32_t(c);  // no hex structure: every cell its own macro cell
+    m.input_cell[c] = order[c];
+  }
+  for (int64_t c = 0; c < n_cells; ++c) {
+    const CellGeometry g = cell_geometry(m, c);
+    SFEM_REQUIRE(std::fabs(g.det) > 0.0 && std::isfinite(g.det), FEM_ERR_ARG,
+                 "mesh: cell " + std::to_string(m.input_cell[c]) + " is degenerate");
+  }
+  build_face_adjacency(m);
   return m;
+}
+
+Mesh read_vtk_mesh(const std::string& path, int reorder) {
+  std::ifstream in(path);
+  SFEM_REQUIRE(in.good(), FEM_ERR_ARG, "vtk: cannot open " + path);
+  std::string line;
+  std::vector<double> x;
+  std::vector<int32_t> cells;
+  std::vector<int> types;
+  int64_t np = -1;
+  bool ascii = false;
+  std::string tok;
+  while (in >> tok) {
+    if (tok == "ASCII") {
+      ascii = true;
+    } else if (tok == "BINARY") {
+      throw Error(FEM_ERR_ARG, "vtk: only ASCII legacy files are read");
+    } else if (tok == "DATASET") {
+      in >> tok;
+      SFEM_REQUIRE(tok == "UNSTRUCTURED_GRID", FEM_ERR_ARG, "vtk: DATASET must be UNSTRUCTURED_GRID");
+    } else if (tok == "POINTS") {
+      std::string type;
+      in >> np >> type;
+      SFEM_REQUIRE(np > 0, FEM_ERR_ARG, "vtk: bad POINTS count");
+      x.resize(3 * np);
+      for (auto& v : x) SFEM_REQUIRE(bool(in >> v), FEM_ERR_ARG, "vtk: short POINTS section");
+    } else if (tok == "CELLS") {
+      int64_t nc = 0, size = 0;
+      in >> nc >> size;
+      SFEM_REQUIRE(nc > 0 && size >= 5 * nc, FEM_ERR_ARG, "vtk: bad CELLS header");
+      cells.reserve(4 * nc);
+      for (int64_t c = 0; c < nc; ++c) {
+        int64_t k = 0;
+        SFEM_REQUIRE(bool(in >> k), FEM_ERR_ARG, "vtk: short CELLS section");
+        SFEM_REQUIRE(k == 4, FEM_ERR_ARG, "vtk: only tetrahedra (4 vertices per cell) are read");
+        for (int v = 0; v < 4; ++v) {
+          int64_t id = 0;
+          SFEM_REQUIRE(bool(in >> id), FEM_ERR_ARG, "vtk: short CELLS section");
+          cells.push_back(int32_t(id));
+        }
+      }
+    } else if (tok == "CELL_TYPES") {
+      int64_t nt = 0;
+      in >> nt;
+      types.resize(nt);
+      for (auto& t : types) SFEM_REQUIRE(bool(in >> t), FEM_ERR_ARG, "vtk: short CELL_TYPES section");
+    } else if (tok == "CELL_DATA" || tok == "POINT_DATA") {
+      break;  // attached data is not needed
+    }
+  }
+  SFEM_REQUIRE(ascii, FEM_ERR_ARG, "vtk: not an ASCII legacy VTK file");
+  SFEM_REQUIRE(np > 0 && !cells.empty(), FEM_ERR_ARG, "vtk: POINTS and CELLS are required");
+  SFEM_REQUIRE(types.empty() || int64_t(types.size()) * 4 == int64_t(cells.size()), FEM_ERR_ARG,
+               "vtk: CELL_TYPES count differs from CELLS");
+  for (int t : types) SFEM_REQUIRE(t == 10, FEM_ERR_ARG, "vtk: only VTK_TETRA (type 10) cells are read");
+  return build_mesh_from_arrays(np, x.data(), int64_t(cells.size() / 4), cells.data(), reorder);
 }
 
 CellGeometry cell_geometry(const Mesh& m, int64_t c) {

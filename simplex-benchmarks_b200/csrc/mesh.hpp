@@ -21,6 +21,7 @@
 #pragma once
 #include <array>
 #include <cstdint>
+#include <string>
 #include <vector>
 
 namespace sfem {
@@ -44,6 +45,8 @@ struct Mesh {
   std::vector<int8_t> nbf;          // [n_cells][4] local face index of f inside the neighbour
   int64_t n_interior_faces = 0;
   int64_t n_boundary_faces = 0;
+  bool structured = false;          // a Kuhn box (hex / cube kernels, h-multigrid)
+  std::vector<int64_t> input_cell;  // meshes from arrays: input index of every cell
 
   // lexicographic vertex index of lattice point (i,j,k)
   int64_t vertex_id(int i, int j, int k) const {
@@ -56,6 +59,19 @@ struct Mesh {
 };
 
 Mesh build_kuhn_mesh(const MeshDescription& d);
+
+// Face neighbours (nb, nbf) and face counts of a mesh with sorted cell vertices.
+void build_face_adjacency(Mesh& m);
+
+// Unstructured tetrahedral mesh from vertex and cell arrays (any vertex order
+// per cell; the cells are stored with sorted vertices).  reorder = 1 puts the
+// cells in Morton order of their centroids, 0 keeps the input order.
+Mesh build_mesh_from_arrays(int64_t n_vertices, const double* x, int64_t n_cells, const int32_t* cells,
+                            int reorder);
+
+// Legacy ASCII VTK unstructured grid (POINTS, CELLS, CELL_TYPES; tetrahedra,
+// VTK cell type 10, only), the format GridIn::read_vtk reads in the reference.
+Mesh read_vtk_mesh(const std::string& path, int reorder);
 
 // Affine geometry of one tet: J = [x1-x0, x2-x0, x3-x0] (J_ij = dx_i/dxi_j).
 struct CellGeometry {

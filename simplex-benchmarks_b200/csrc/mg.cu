@@ -476,6 +476,8 @@ class MultigridImpl final : public Multigrid {
     SFEM_REQUIRE(prm.c_transfer == 0 || prm.c_transfer == 1, FEM_ERR_ARG, "multigrid: c_transfer must be 0 or 1");
     SFEM_REQUIRE(prm.smoother_degree >= 1 && prm.smoother_degree <= 32, FEM_ERR_ARG, "multigrid: smoother degree");
     const Mesh& mf = *fine.mesh;
+    SFEM_REQUIRE(mf.structured, FEM_ERR_ARG,
+                 "multigrid: the h-levels need a Kuhn box mesh (fem_mesh_create), not a mesh from arrays");
     fine_m_ = fine.m;
     // number of h-levels
     int H = 0;

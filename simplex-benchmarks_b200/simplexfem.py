@@ -82,6 +82,10 @@ _PROTOS = [
     ("fem_last_error_string", C.c_char_p, []),
     ("fem_version", C.c_int, [C.POINTER(C.c_int32), C.POINTER(C.c_int32)]),
     ("fem_mesh_create", C.c_int, [C.POINTER(MeshDesc), C.POINTER(C.c_void_p)]),
+    ("fem_mesh_create_from_arrays", C.c_int, [C.c_int64, C.c_void_p, C.c_int64, C.c_void_p, C.c_int32,
+                                              C.POINTER(C.c_void_p)]),
+    ("fem_mesh_read_vtk", C.c_int, [C.c_char_p, C.c_int32, C.POINTER(C.c_void_p)]),
+    ("fem_mesh_copy_input_cells", C.c_int, [C.c_void_p, C.c_void_p]),
     ("fem_mesh_destroy", C.c_int, [C.c_void_p]),
     ("fem_mesh_sizes", C.c_int, [C.c_void_p] + [C.POINTER(C.c_int64)] * 4),
     ("fem_mesh_copy_vertices", C.c_int, [C.c_void_p, C.c_void_p]),
@@ -210,12 +214,45 @@ class Mesh:
         d.seed = seed
         h = C.c_void_p()
         check(lib().fem_mesh_create(C.byref(d), C.byref(h)))
-        self.handle = h
+        self._adopt(h)
         self.n, self.lo, self.hi, self.jitter, self.seed = tuple(n), tuple(lo), tuple(hi), jitter, seed
+
+    def _adopt(self, h):
+        self.handle = h
         nv, nc, fi, fb = (C.c_int64() for _ in range(4))
         check(lib().fem_mesh_sizes(h, C.byref(nv), C.byref(nc), C.byref(fi), C.byref(fb)))
         self.n_vertices, self.n_cells = nv.value, nc.value
         self.n_interior_faces, self.n_boundary_faces = fi.value, fb.value
+
+    @classmethod
+    def from_arrays(cls, vertices, cells, reorder=True):
+        """Unstructured tet mesh (fem_mesh_create_from_arrays); reorder puts the
+        cells in Morton order of their centroids."""
+        x = np.ascontiguousarray(vertices, np.float64)
+        c = np.ascontiguousarray(cells, np.int32)
+        h = C.c_void_p()
+        check(lib().fem_mesh_create_from_arrays(len(x), x.ctypes.data, len(c), c.ctypes.data, int(bool(reorder)),
+                                                C.byref(h)))
+        m = cls.__new__(cls)
+        m._adopt(h)
+        m.n = None
+        return m
+
+    @classmethod
+    def read_vtk(cls, path, reorder=True):
+        """Legacy ASCII VTK unstructured grid of tetrahedra (fem_mesh_read_vtk)."""
+        h = C.c_void_p()
+        check(lib().fem_mesh_read_vtk(os.fsencode(str(path)), int(bool(reorder)), C.byref(h)))
+        m = cls.__new__(cls)
+        m._adopt(h)
+        m.n = None
+        return m
+
+    def input_cells(self):
+        """Input index of every cell (meshes from arrays; identity otherwise)."""
+        a = np.empty(self.n_cells, np.int64)
+        check(lib().fem_mesh_copy_input_cells(self.handle, a.ctypes.data))
+        return a
 
     def vertices(self):
         a = np.empty((self.n_vertices, 3), np.float64)
