@@ -711,6 +711,37 @@ int fast_info(const fast_ctx* ctx, int32_t* nq, int32_t* nqf, int32_t* lanes, in
   return 0;
 }
 
+// diagonal of the CG operator (constrained rows 1): sum over cells of
+// w_q (D_q phi_i)^T G (D_q phi_i), the Jacobi entries of the smoother
+int fast_diagonal(fast_ctx* ctx, double* diag) {
+  Ctx& c = *reinterpret_cast<Ctx*>(ctx);
+  if (c.prm.kind != KIND_CG) return 1;
+  const int K = c.K, nq = c.nq;
+  // per local node i and metric component k: sum_q w_q g_a g_b
+  std::vector<double> S(size_t(K) * 6, 0.0);
+  const int ia[6] = {0, 1, 2, 0, 0, 1}, ib[6] = {0, 1, 2, 1, 2, 2};
+  for (int i = 0; i < K; ++i)
+    for (int q = 0; q < nq; ++q)
+      for (int k = 0; k < 6; ++k) {
+        const double ga = c.D[(size_t(q) * 3 + ia[k]) * K + i], gb = c.D[(size_t(q) * 3 + ib[k]) * K + i];
+        S[size_t(i) * 6 + k] += c.wq[q] * ga * gb * (ia[k] == ib[k] ? 1.0 : 2.0);
+      }
+  std::fill(diag, diag + c.n_dofs, 0.0);
+  for (int64_t b = 0; b < c.n_batches; ++b)
+    for (int v = 0; v < L; ++v) {
+      if (c.bcell[b * L + v] < 0) continue;
+      for (int i = 0; i < K; ++i) {
+        const int32_t d = c.bdofs[(b * K + i) * L + v];
+        if (d < 0) continue;
+        double s = 0;
+        for (int k = 0; k < 6; ++k) s += S[size_t(i) * 6 + k] * c.metric[6 * b + k][v];
+        diag[d] += s;
+      }
+    }
+  for (int32_t d : c.constrained_list) diag[d] = 1.0;
+  return 0;
+}
+
 int fast_vmult(fast_ctx* ctx, const double* src, double* dst) {
   Ctx& c = *reinterpret_cast<Ctx*>(ctx);
   const int p = c.prm.degree;

@@ -46,6 +46,8 @@ def lib():
         L.fast_n_dofs.argtypes = [C.c_void_p]
         L.fast_info.argtypes = [C.c_void_p] + [C.POINTER(C.c_int32)] * 4
         L.fast_vmult.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p]
+        L.fast_diagonal.restype = C.c_int
+        L.fast_diagonal.argtypes = [C.c_void_p, C.c_void_p]
         _lib = L
     return _lib
 
@@ -86,6 +88,13 @@ class FastOperator:
             dst = np.empty(self.n, np.float64)
         lib().fast_vmult(self.h, src.ctypes.data, dst.ctypes.data)
         return dst
+
+    def diagonal(self):
+        """CG only: the operator's diagonal (1 on constrained rows)."""
+        d = np.empty(self.n, np.float64)
+        if lib().fast_diagonal(self.h, d.ctypes.data) != 0:
+            raise RuntimeError("fast_diagonal: CG operators only")
+        return d
 
     def __del__(self):
         if getattr(self, "h", None) and _lib is not None:

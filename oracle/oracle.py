@@ -138,6 +138,7 @@ class KuhnMesh:
         if isinstance(n, int):
             n = (n, n, n)
         self.n = tuple(int(v) for v in n)
+        self.lo, self.hi, self.jitter, self.seed = tuple(lo), tuple(hi), jitter, seed
         nv = (self.n[0] + 1) * (self.n[1] + 1) * (self.n[2] + 1)
         self.n_vertices = nv
         self.n_cells = 6 * self.n[0] * self.n[1] * self.n[2]

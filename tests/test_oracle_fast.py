@@ -52,3 +52,24 @@ def test_fast_port_rules_are_small():
     QGaussSimplex(p+1): 14 cell and 12 face points for DG P3."""
     f = fast.FastOperator(orc.KuhnMesh(2), 3, orc.DG)
     assert (f.n_cell_points, f.n_face_points, f.lanes) == (14, 12, 8)
+
+
+@pytest.mark.parametrize("p", [2, 3])
+def test_fast_multigrid_equals_assembled_oracle(p):
+    """The matrix-free CPU multigrid (oracle/fast_mg.py, the timed CPU solve
+    baseline) gives the same V-cycle as the assembled restatement
+    (mg_oracle.MGOracle) and the same MG-CG iteration count to 1e-8."""
+    import torch
+    import fast_mg
+    import mg_oracle
+    mg = fast_mg.FastMG(8, p)
+    mo = mg_oracle.MGOracle(lambda k: orc.KuhnMesh(k), 8, p)
+    L = mg.levels[-1]
+    b = np.random.default_rng(5).uniform(-1, 1, L.n)
+    b[L.constrained.numpy()] = 0.0
+    z = mg.vcycle(torch.from_numpy(b.copy())).numpy()
+    assert rel_l2(z, mo.vcycle(b)) <= 1e-12
+    _, its = mg.solve(torch.from_numpy(b.copy()), rtol=1e-8)
+    A = mo.levels[-1].A
+    _, its_ref = mg_oracle.pcg(lambda v: A @ v, b, mo.vcycle, 1e-8, 100)
+    assert its == its_ref
