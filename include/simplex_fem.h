@@ -99,7 +99,12 @@ typedef struct fem_op_params {
                               FP32 on the TF32 tensor cores per cube (the cube kernel
                               with each tile of 128 tets as one tcgen05 product;
                               variant 4 on meshes without whole cubes) */
-  int32_t reserved[5];
+  int32_t weak_boundary;   /* FEM_CG: 1 = weak (Nitsche) homogeneous Dirichlet on the boundary
+                              faces (2 sigma u v - d_n u v - u d_n v, sigma = (p+1)(p+3)/3 *
+                              surface/volume) and no constrained DoFs, as the CG levels of the
+                              reference's DG multigrid (DG/cells_batched/application_phc.cc:
+                              1799-1832); 0 = strong constraints (default) */
+  int32_t reserved[4];
 } fem_op_params;
 
 /* ---- library ----------------------------------------------------------- */
@@ -289,7 +294,10 @@ typedef struct fem_mg_params {
   int32_t tensor_cores;     /* FP32 CG levels apply their operator with TF32 tensor-core
                                contractions (kernel variant 8: per cube, or per cell on
                                levels without whole cubes; operator accurate to ~1e-3) */
-  int32_t reserved[1];
+  int32_t weak_cg_levels;   /* FEM_DG fine operators: 1 = the CG levels use weak boundary terms
+                               and no constrained DoFs (the reference's phc/cph/chp hierarchy,
+                               DG/cells_batched/application_phc.cc:1737-1744,1799-1832);
+                               0 = strong Dirichlet constraints (default) */
 } fem_mg_params;
 int fem_mg_params_default(fem_mg_params* p);
 int fem_mg_create(fem_op* fine, const fem_mg_params* p, fem_mg** out);

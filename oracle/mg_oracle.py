@@ -49,11 +49,16 @@ def lattice_nodes(p):
 
 
 class Level:
-    def __init__(self, mesh, p):
+    def __init__(self, mesh, p, weak=False):
+        """weak: boundary imposed by Nitsche terms, no constrained DoFs (the CG
+        levels of DG/cells_batched/application_phc.cc:1799-1832)."""
         self.mesh, self.p = mesh, p
         self.cd, self.cm = mesh.cg_dofs(p)
+        if weak:
+            self.cm = np.zeros_like(self.cm)
         self.n = len(self.cm)
-        o = orc.Oracle(mesh.vertices(), mesh.cells(), p, orc.CG, cell_dofs=self.cd, constrained=self.cm)
+        o = orc.Oracle(mesh.vertices(), mesh.cells(), p, orc.CG, cell_dofs=self.cd, constrained=self.cm,
+                       weak_bc=weak)
         K = self.cd.shape[1]
         rows, cols, vals = [], [], []
         free = ~self.cm.astype(bool)
@@ -119,7 +124,7 @@ def transfer(fine, coarse):
 
 class MGOracle:
     def __init__(self, make_mesh, n, p, order="ph", coarse_n=4, degree=3, smoothing_range=20.0,
-                 eig_iterations=10, eig_safety=1.2, seed=0):
+                 eig_iterations=10, eig_safety=1.2, seed=0, weak=False):
         H = int(round(np.log2(n // coarse_n)))
         meshes = [make_mesh(n >> k) for k in range(H + 1)]  # fine .. coarse
         seq = []
@@ -129,7 +134,7 @@ class MGOracle:
         else:
             seq += [(meshes[H], q) for q in range(1, p + 1)]
             seq += [(meshes[k], p) for k in range(H - 1, -1, -1)]
-        self.levels = [Level(m, q) for (m, q) in seq]
+        self.levels = [Level(m, q, weak) for (m, q) in seq]
         self.P = [None] + [transfer(self.levels[l], self.levels[l - 1]) for l in range(1, len(self.levels))]
         self.degree = degree
         rng = np.random.default_rng(seed)
@@ -246,14 +251,15 @@ class DGMGOracle(MGOracle):
     P_pc on the same mesh (continuous nodal values copied into every cell,
     constrained nodes as 0), then the CG ladder of MGOracle.  pc = 1
     (c_transfer 0, phc) or p (c_transfer 1, cph / chp).  The CG levels keep the
-    strong homogeneous Dirichlet constraints of the CG operator."""
+    strong homogeneous Dirichlet constraints of the CG operator, or with
+    weak_cg take the reference's weak boundary terms and no constraints."""
 
     def __init__(self, make_mesh, n, p, c_transfer=0, order="ph", coarse_n=4, degree=3, smoothing_range=20.0,
-                 eig_iterations=10, eig_safety=1.2, seed=0):
+                 eig_iterations=10, eig_safety=1.2, seed=0, weak_cg=False):
         pc = 1 if c_transfer == 0 else p
         super().__init__(make_mesh, n, pc, order=order, coarse_n=coarse_n, degree=degree,
                          smoothing_range=smoothing_range, eig_iterations=eig_iterations, eig_safety=eig_safety,
-                         seed=seed)
+                         seed=seed, weak=weak_cg)
         mesh = make_mesh(n)
         cgtop = self.levels[-1]
         rng = np.random.default_rng(seed + 1)

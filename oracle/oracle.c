@@ -335,7 +335,10 @@ int oracle_create(const oracle_params* prm, int64_t nv, const double* x, int64_t
     ctx->cell_dofs = (int32_t*)malloc(sizeof(int32_t) * K * nc);
     memcpy(ctx->cell_dofs, cell_dofs, sizeof(int32_t) * K * nc);
     ctx->constrained = (uint8_t*)malloc(n_dofs);
-    memcpy(ctx->constrained, constrained, n_dofs);
+    if (prm->weak_bc)
+      memset(ctx->constrained, 0, n_dofs); /* the boundary is imposed weakly */
+    else
+      memcpy(ctx->constrained, constrained, n_dofs);
   } else {
     ctx->ndofs = (int64_t)K * ctx->prm.n_components * nc;
   }
@@ -436,12 +439,13 @@ static void cell_apply(const oracle_ctx* ctx, int64_t c, const double* u /* [nc]
       }
     }
   }
-  if (!dg) return;
-  /* face terms, own side */
+  if (!dg && !ctx->prm.weak_bc) return;
+  /* face terms, own side (weak CG: the boundary faces only) */
   for (int f = 0; f < 4; ++f) {
+    const int32_t nbc = ctx->nb[4 * c + f];
+    if (!dg && nbc >= 0) continue;
     double P0[3], E1[3], E2[3], n[3], area;
     face_frame(ctx, c, f, P0, E1, E2, n, &area);
-    const int32_t nbc = ctx->nb[4 * c + f];
     double sigma;
     if (helm)
       sigma = nbc >= 0 ? ctx->factor * 0.5 * (ctx->ih[4 * c + f] + ctx->ih[4 * (int64_t)nbc + ctx->nbf[4 * c + f]])

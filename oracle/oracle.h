@@ -47,6 +47,8 @@ typedef struct oracle_params {
   double mass;          /* Helmholtz mass coefficient */
   int32_t quad_points;  /* Gauss points per collapsed direction (0: degree + 2) */
   int32_t n_threads;    /* OpenMP threads (0: all) */
+  int32_t weak_bc;      /* CG: weak (Nitsche) homogeneous Dirichlet on boundary faces, no constrained
+                           DoFs (the CG levels of DG/cells_batched/application_phc.cc:1799-1832) */
 } oracle_params;
 
 typedef struct oracle_ctx oracle_ctx;

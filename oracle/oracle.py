@@ -17,7 +17,7 @@ CG, DG, HELMHOLTZ = 0, 1, 2
 class Params(C.Structure):
     _fields_ = [("degree", C.c_int32), ("kind", C.c_int32), ("n_components", C.c_int32),
                 ("penalty", C.c_int32), ("mass", C.c_double), ("quad_points", C.c_int32),
-                ("n_threads", C.c_int32)]
+                ("n_threads", C.c_int32), ("weak_bc", C.c_int32)]
 
 
 _lib = None
@@ -61,10 +61,10 @@ class Oracle:
     """FP64 CPU operator on the same mesh arrays as the product."""
 
     def __init__(self, x, cells, degree, kind, cell_dofs=None, constrained=None, n_components=1,
-                 penalty=0, mass=1e5, quad_points=0, n_threads=0):
+                 penalty=0, mass=1e5, quad_points=0, n_threads=0, weak_bc=False):
         self.x = np.ascontiguousarray(x, np.float64)
         self.cells = np.ascontiguousarray(cells, np.int32)
-        p = Params(degree, kind, n_components, penalty, mass, quad_points, n_threads)
+        p = Params(degree, kind, n_components, penalty, mass, quad_points, n_threads, int(bool(weak_bc)))
         self.kind = kind
         if kind == CG:
             self.cell_dofs = np.ascontiguousarray(cell_dofs, np.int32)

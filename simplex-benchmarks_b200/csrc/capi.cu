@@ -161,6 +161,9 @@ OpConfig op_config(int32_t degree, int32_t kind, int32_t precision, const fem_op
       }
       cfg.penalty = params->penalty;
       cfg.kernel_variant = params->kernel_variant;
+      SFEM_REQUIRE(params->weak_boundary == 0 || (params->weak_boundary == 1 && kind == FEM_CG), FEM_ERR_ARG,
+                   "weak_boundary must be 0, or 1 for FEM_CG operators");
+      cfg.weak_bc = params->weak_boundary == 1;
       SFEM_REQUIRE(valid_variant(kind, cfg.kernel_variant), FEM_ERR_ARG,
                    "kernel_variant must be 0..8 (CG) or 0..5, 7, 9, 11 (DG, Helmholtz)");
       SFEM_REQUIRE((cfg.kernel_variant != 4 && cfg.kernel_variant != 8) || kind != FEM_CG || precision == FEM_FP32,

@@ -83,6 +83,7 @@ int fem_mg_params_default(fem_mg_params* p) {
     p->c_transfer = d.c_transfer;
     p->learned_steps = d.learned_steps;
     p->tensor_cores = d.tensor_cores;
+    p->weak_cg_levels = d.weak_cg_levels;
   });
 }
 
@@ -103,7 +104,10 @@ int fem_mg_create(fem_op* fine, const fem_mg_params* p, fem_mg** out) {
       prm.c_transfer = p->c_transfer;
       prm.learned_steps = p->learned_steps;
       prm.tensor_cores = p->tensor_cores;
+      prm.weak_cg_levels = p->weak_cg_levels;
     }
+    SFEM_REQUIRE(prm.weak_cg_levels == 0 || (prm.weak_cg_levels == 1 && fine->op->cfg.kind == FEM_DG), FEM_ERR_ARG,
+                 "mg: weak_cg_levels must be 0, or 1 for a FEM_DG fine operator");
     SFEM_REQUIRE(prm.learned_steps >= 1 && prm.learned_steps <= 3, FEM_ERR_ARG, "mg: learned_steps must be 1..3");
     SFEM_REQUIRE(prm.order == FEM_MG_PH || prm.order == FEM_MG_HP, FEM_ERR_ARG, "mg: order must be PH or HP");
     SFEM_REQUIRE(prm.eig_iterations >= 1 && prm.smoothing_range > 1 && prm.eig_safety >= 1, FEM_ERR_ARG,

@@ -480,6 +480,92 @@ __global__ void __launch_bounds__(BS, 1) dg_apply_xp_kernel(const __grid_constan
   }
 }
 
+// Weak homogeneous Dirichlet terms of a CG operator on boundary face F of
+// each listed cell (the CG levels of the reference's DG multigrid,
+// DG/cells_batched/application_phc.cc:1799-1832): test by value 2 sigma u -
+// d_n u, test by normal derivative -u, with sf = sigma |F|.  One thread per
+// boundary face; the cell's DoFs come from the CG table [K][n_cells] and the
+// results are added atomically.  diag: the diagonal of those terms instead
+// (each local basis function applied on its own, x unused).
+template <int P, int F, typename T>
+__global__ void __launch_bounds__(128) cg_weak_boundary_kernel(int64_t n, const int32_t* __restrict__ cells,
+                                                               const T* __restrict__ sfs, int64_t n_cells,
+                                                               const int32_t* __restrict__ dofs,
+                                                               const T* __restrict__ geo, const T* __restrict__ x,
+                                                               T* __restrict__ dst, bool diag) {
+  using O = gen::Ops<P>;
+  constexpr int K = O::K, KQ = O::KQ, NF = O::NF, NFQ = O::NFQ;
+  const int64_t e = blockIdx.x * int64_t(blockDim.x) + threadIdx.x;
+  if (e >= n) return;
+  const int64_t c = cells[e];
+  const T sf = sfs[e];
+  T G[6];
+#pragma unroll
+  for (int k = 0; k < 6; ++k) G[k] = geo[k * n_cells + c];
+  T cf[3];
+  face_cf(G, F, cf);
+  int32_t dof[K];
+#pragma unroll
+  for (int i = 0; i < K; ++i) dof[i] = dofs[int64_t(i) * n_cells + c];
+  // y = B u for the local boundary operator B of face F
+  auto apply = [&](const T (&u)[K], T (&y)[K]) {
+    T g[3 * KQ];
+    O::grad(u, g);
+    T j[NF], avg[NFQ];
+#pragma unroll
+    for (int i = 0; i < NF; ++i) j[i] = T(2) * u[O::fn(F, i)];
+#pragma unroll
+    for (int m = 0; m < NFQ; ++m) {
+      const int nq = O::fnq(F, m);
+      avg[m] = T(-0.5) * (cf[0] * g[nq] + cf[1] * g[KQ + nq] + cf[2] * g[2 * KQ + nq]);
+    }
+    T t[NF];
+    O::facePP(j, t);
+#pragma unroll
+    for (int i = 0; i < NF; ++i) t[i] *= sf;
+    O::facePQ(avg, t);
+#pragma unroll
+    for (int i = 0; i < K; ++i) y[i] = T(0);
+#pragma unroll
+    for (int i = 0; i < NF; ++i) y[O::fn(F, i)] += t[i];
+    T r[NFQ];
+    O::faceQP(j, r);
+    T h[3 * KQ];
+#pragma unroll
+    for (int q = 0; q < 3 * KQ; ++q) h[q] = T(0);
+#pragma unroll
+    for (int m = 0; m < NFQ; ++m) {
+      const int nq = O::fnq(F, m);
+      const T rm = T(-0.25) * r[m];
+      h[nq] += cf[0] * rm;
+      h[KQ + nq] += cf[1] * rm;
+      h[2 * KQ + nq] += cf[2] * rm;
+    }
+    O::gradT(h, y);
+  };
+  if (!diag) {
+    T u[K], y[K];
+#pragma unroll
+    for (int i = 0; i < K; ++i) u[i] = dof[i] >= 0 ? x[dof[i]] : T(0);
+    apply(u, y);
+#pragma unroll
+    for (int i = 0; i < K; ++i)
+      if (dof[i] >= 0) atomicAdd(dst + dof[i], y[i]);
+  } else {
+    for (int i = 0; i < K; ++i) {
+      T u[K], y[K];
+#pragma unroll
+      for (int k = 0; k < K; ++k) u[k] = k == i ? T(1) : T(0);
+      apply(u, y);
+      T yi = T(0);
+#pragma unroll
+      for (int k = 0; k < K; ++k)
+        if (k == i) yi = y[k];
+      if (dof[i] >= 0) atomicAdd(dst + dof[i], yi);
+    }
+  }
+}
+
 // Diagonal of the DG operator: (A)_ii = own-cell terms applied to e_i, with
 // the own traces of e_i formed on the fly and the neighbour traces zero.
 // Set-up only: plain per-thread code, 128 cells per block of work.

@@ -530,6 +530,7 @@ class MultigridImpl final : public Multigrid {
       cfg.degree = L.degree;
       cfg.kind = L.kind;
       cfg.kernel_variant = prm.tensor_cores && L.kind == FEM_CG && cfg.precision == FEM_FP32 ? 8 : 0;
+      cfg.weak_bc = prm.weak_cg_levels && L.kind == FEM_CG;
       L.op = make_operator(*L.mesh, cfg);
       const int64_t m = L.op->m;
       L.inv_diag.alloc(m);

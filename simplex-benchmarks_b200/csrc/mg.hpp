@@ -35,6 +35,9 @@ struct MGParams {
   // FP32 CG levels apply their operator on the TF32 tensor cores
   // (cg_cell_tc_kernel, kernel variant 4)
   int tensor_cores = 0;
+  // DG fine operators: the CG levels take weak (Nitsche) boundary terms and no
+  // constrained DoFs, as in the reference's DG multigrid
+  int weak_cg_levels = 0;
 };
 
 class Multigrid {

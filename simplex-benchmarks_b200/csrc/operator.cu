@@ -512,6 +512,12 @@ class CGOperator final : public Operator {
   // constrained DoFs as identity rows.
   CGOperator(const Mesh& mesh, CGDofs dofs, const std::vector<uint8_t>* identity, const OpConfig& c) {
     cfg = c;
+    if (cfg.weak_bc) {
+      // weak (Nitsche) Dirichlet: no DoF is constrained, boundary faces carry
+      // the penalty terms instead
+      std::fill(dofs.constrained.begin(), dofs.constrained.end(), uint8_t(0));
+      identity = nullptr;
+    }
     K = dofs.K;
     n_cells = mesh.n_cells;
     m = dofs.n_dofs;
@@ -542,6 +548,7 @@ class CGOperator final : public Operator {
     d_constrained.upload(cl);
     build_hex_tables(mesh, dofs, geo);
     build_cube_tables(dofs);
+    if (cfg.weak_bc) build_weak_boundary(mesh);
     d_status.alloc(1);
     SFEM_CUDA(cudaMemset(d_status.p, 0, sizeof(int)));
     if (std::is_same<T, float>::value && n_cells > 0) {
@@ -601,6 +608,65 @@ class CGOperator final : public Operator {
       SFEM_CUDA(cudaMemsetAsync(d, 0, sizeof(T) * m, s));
       return;
     }
+    apply_cells(x, d, s);
+    if (cfg.weak_bc) apply_boundary(x, d, false, s);
+  }
+
+  // weak (Nitsche) boundary terms: boundary faces grouped by local face number
+  DevBuf<int32_t> d_bcell[4];
+  DevBuf<T> d_bsf[4];
+
+  void build_weak_boundary(const Mesh& mesh) {
+    const int p = cfg.degree;
+    const double factor = double((p + 1) * (p + 3)) / 3.0;
+    std::vector<int32_t> cells[4];
+    std::vector<T> sf[4];
+    for (int64_t cc = 0; cc < n_cells; ++cc) {
+      const double vol = std::fabs(cell_geometry(mesh, cc).det) / 6.0;
+      double area[4], surf = 0;
+      for (int f = 0; f < 4; ++f) {
+        double nrm[3];
+        face_area_normal(mesh, cc, f, area[f], nrm);
+        surf += area[f] * (mesh.nb[4 * cc + f] == -1 ? 1.0 : 0.5);
+      }
+      const double tau = surf / vol;  // surface / volume (DG/cells_batched/application_phc.cc:1284-1313)
+      for (int f = 0; f < 4; ++f)
+        if (mesh.nb[4 * cc + f] == -1) {
+          cells[f].push_back(int32_t(cc));
+          sf[f].push_back(T(factor * tau * area[f]));
+        }
+    }
+    for (int f = 0; f < 4; ++f) {
+      d_bcell[f].upload(cells[f]);
+      d_bsf[f].upload(sf[f]);
+    }
+  }
+
+  template <int P>
+  void launch_boundary(const T* x, T* d, bool diag, cudaStream_t s) {
+    auto go = [&](auto fc) {
+      constexpr int F = decltype(fc)::value;
+      const int64_t nb = int64_t(d_bcell[F].n);
+      if (!nb) return;
+      cg_weak_boundary_kernel<P, F, T><<<blocks_for(nb, 128), 128, 0, s>>>(nb, d_bcell[F].p, d_bsf[F].p, n_cells,
+                                                                          d_dofs.p, d_geo.p, x, d, diag);
+    };
+    go(std::integral_constant<int, 0>{});
+    go(std::integral_constant<int, 1>{});
+    go(std::integral_constant<int, 2>{});
+    go(std::integral_constant<int, 3>{});
+  }
+
+  void apply_boundary(const T* x, T* d, bool diag, cudaStream_t s) {
+    switch (cfg.degree) {
+      case 1: launch_boundary<1>(x, d, diag, s); break;
+      case 2: launch_boundary<2>(x, d, diag, s); break;
+      case 3: launch_boundary<3>(x, d, diag, s); break;
+    }
+    SFEM_CUDA(cudaGetLastError());
+  }
+
+  void apply_cells(const T* x, T* d, cudaStream_t s) {
     // default (variant 0), measured on B200: P1 per cube in FP64 and per hex
     // in FP32, P2 per cube, P3 per cube in FP32 and per cell in FP64; per cell on meshes too small to give
     // every SM two cubes (or two CTAs of hexes), where the coarser forms
@@ -682,6 +748,7 @@ class CGOperator final : public Operator {
       case 3: cg_diagonal_kernel<3, T><<<grid, 128, 0, s>>>(n_cells, d_dofs.p, d_geo.p, d, d_constrained.n, d_constrained.p); break;
     }
     SFEM_CUDA(cudaGetLastError());
+    if (cfg.weak_bc) apply_boundary(nullptr, d, true, s);
   }
 
   const int32_t* device_dof_table() const override { return d_dofs.p; }

@@ -62,6 +62,7 @@ struct OpConfig {
   int n_components = 1;
   int penalty = FEM_PENALTY_REFERENCE;
   int kernel_variant = 0;  // 0: tuned default (see fem_op_params.kernel_variant)
+  bool weak_bc = false;    // CG: weak (Nitsche) Dirichlet on the boundary faces, no constrained DoFs
 };
 
 struct HostPipe;  // staging buffers and streams of vmult_host (host_vmult.cu)

@@ -38,7 +38,8 @@ class MeshDesc(C.Structure):
 
 class OpParams(C.Structure):
     _fields_ = [("mass_coefficient", C.c_double), ("n_components", C.c_int32),
-                ("penalty", C.c_int32), ("kernel_variant", C.c_int32), ("reserved", C.c_int32 * 5)]
+                ("penalty", C.c_int32), ("kernel_variant", C.c_int32), ("weak_boundary", C.c_int32),
+                ("reserved", C.c_int32 * 4)]
 
 
 class RhsDesc(C.Structure):
@@ -50,7 +51,7 @@ class MGParams(C.Structure):
     _fields_ = [("order", C.c_int32), ("precision", C.c_int32), ("smoother_degree", C.c_int32),
                 ("eig_iterations", C.c_int32), ("smoothing_range", C.c_double), ("eig_safety", C.c_double),
                 ("coarse_n", C.c_int32), ("use_graph", C.c_int32), ("c_transfer", C.c_int32),
-                ("learned_steps", C.c_int32), ("tensor_cores", C.c_int32), ("reserved", C.c_int32 * 1)]
+                ("learned_steps", C.c_int32), ("tensor_cores", C.c_int32), ("weak_cg_levels", C.c_int32)]
 
 
 class SolveInfo(C.Structure):
@@ -289,7 +290,7 @@ class Operator:
     """Matrix-free operator (fem_op); the drop-in for the reference's Operator."""
 
     def __init__(self, mesh, degree, kind="cg", precision="fp64", mass=1e5, n_components=None,
-                 penalty=FEM_PENALTY_REFERENCE, partition=None):
+                 penalty=FEM_PENALTY_REFERENCE, partition=None, weak_boundary=False):
         """partition: a Partition of `mesh`; the operator is then that part's
         local operator on [owned | ghost] vectors (fem_op_create_part)."""
         self.mesh = mesh
@@ -299,6 +300,7 @@ class Operator:
         p.mass_coefficient = mass
         p.n_components = n_components or (3 if k == FEM_HELMHOLTZ else 1)
         p.penalty = penalty
+        p.weak_boundary = int(bool(weak_boundary))
         h = C.c_void_p()
         if partition is None:
             check(lib().fem_op_create(mesh.handle, degree, k, pr, C.byref(p), C.byref(h)))
@@ -526,11 +528,12 @@ def interpolate(op, desc, dst=None, stream=None):
 class Multigrid:
     """Hybrid p/h/c multigrid on a CG or DG operator (fem_mg); MultigridPreconditioner's shape.
     DG: c_transfer=0 coarsens DG P_p .. P_1 then hands over to CG P_1 (phc);
-    c_transfer=1 hands over at P_p (cph with FEM_MG_PH, chp with FEM_MG_HP)."""
+    c_transfer=1 hands over at P_p (cph with FEM_MG_PH, chp with FEM_MG_HP);
+    weak_cg_levels gives the CG levels weak boundary terms (the reference's)."""
 
     def __init__(self, fine_op, order=FEM_MG_PH, precision="fp32", smoother_degree=3, smoothing_range=20.0,
                  eig_iterations=10, eig_safety=1.2, coarse_n=4, use_graph=True, c_transfer=0, learned_steps=3,
-                 tensor_cores=False):
+                 tensor_cores=False, weak_cg_levels=False):
         p = MGParams()
         check(lib().fem_mg_params_default(C.byref(p)))
         p.order = order
@@ -544,6 +547,7 @@ class Multigrid:
         p.c_transfer = c_transfer
         p.learned_steps = learned_steps
         p.tensor_cores = int(bool(tensor_cores))
+        p.weak_cg_levels = int(bool(weak_cg_levels))
         h = C.c_void_p()
         check(lib().fem_mg_create(fine_op.handle, C.byref(p), C.byref(h)))
         self.handle = h

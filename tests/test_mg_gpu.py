@@ -178,15 +178,18 @@ def test_config3_full_size(cuda):
 
 @pytest.mark.parametrize("p,c_transfer,order", [(2, 0, sf.FEM_MG_PH), (3, 0, sf.FEM_MG_PH),
                                                 (3, 1, sf.FEM_MG_PH), (3, 1, sf.FEM_MG_HP)])
-def test_dg_multigrid_iterations_match_oracle(cuda, p, c_transfer, order):
+@pytest.mark.parametrize("weak", [False, True])
+def test_dg_multigrid_iterations_match_oracle(cuda, p, c_transfer, order, weak):
     """DG (SIPG) P_p solved by CG with the p/c/h multigrid (phc: DG P_p .. P_1,
     CG P_1, h-levels; cph/chp: CG P_p right below DG P_p): iteration count to
-    1e-8 within +-1 of the CPU oracle's multigrid on the same problem."""
+    1e-8 within +-1 of the CPU oracle's multigrid on the same problem.  weak:
+    the CG levels carry the reference's weak boundary terms and no constrained
+    DoFs (DG/cells_batched/application_phc.cc:1737-1744,1799-1832)."""
     import torch
     n = 4
     mesh = sf.Mesh(n)
     op = sf.Operator(mesh, p, "dg")
-    mg = sf.Multigrid(op, order=order, precision="fp64", coarse_n=2, c_transfer=c_transfer)
+    mg = sf.Multigrid(op, order=order, precision="fp64", coarse_n=2, c_transfer=c_transfer, weak_cg_levels=weak)
     kinds = [mg.level_info(l)["kind"] for l in range(mg.n_levels)]
     assert kinds[-1] == "dg" and kinds[0] == "cg"
     assert kinds.count("dg") == (p if c_transfer == 0 else 1)
@@ -197,7 +200,7 @@ def test_dg_multigrid_iterations_match_oracle(cuda, p, c_transfer, order):
     res = sf.SolverCG(op, mg).solve(x, b, rtol=1e-8, max_iterations=100)
     assert res["status"] == sf.FEM_OK, res
     M = mgo.DGMGOracle(lambda k: sf.Mesh(k), n, p, c_transfer=c_transfer,
-                       order="ph" if order == sf.FEM_MG_PH else "hp", coarse_n=2)
+                       order="ph" if order == sf.FEM_MG_PH else "hp", coarse_n=2, weak_cg=weak)
     top = M.levels[-1]
     _, its = mgo.pcg(lambda v: top.A @ v, bh, M.vcycle, 1e-8, 100)
     assert abs(res["iterations"] - its) <= 1, (res["iterations"], its)
@@ -220,3 +223,26 @@ def test_mg_with_tf32_tensor_core_levels(cuda):
         assert r["status"] == sf.FEM_OK, r
         its[tc] = r["iterations"]
     assert its[True] <= its[False] + 2, its
+
+
+@pytest.mark.parametrize("variant", [0, 1, 2, 3, 5, 6, 7])
+@pytest.mark.parametrize("p", [1, 2, 3])
+def test_cg_weak_boundary_operator(cuda, p, variant):
+    """CG operator with weak (Nitsche) boundary terms and no constrained DoFs
+    (fem_op_params.weak_boundary), every cell-kernel form plus the boundary
+    kernel, and its diagonal, against the oracle's weak mode (FP64, 1e-12)."""
+    import torch
+    mesh = sf.Mesh((8, 8, 4), jitter=0.1, seed=6)
+    op = sf.Operator(mesh, p, "cg", "fp64", weak_boundary=True)
+    assert op.constrained().sum() == 0
+    op.set_kernel_variant(variant)
+    cd, cm = mesh.cg_dofs(p)
+    o = orc.Oracle(mesh.vertices(), mesh.cells(), p, orc.CG, cell_dofs=cd, constrained=cm, weak_bc=True)
+    x = np.random.default_rng(3).uniform(-1, 1, op.m())
+    y = op.initialize_dof_vector()
+    op.vmult(y, torch.tensor(x, device="cuda"))
+    d = op.initialize_dof_vector()
+    op.compute_diagonal(d)
+    torch.cuda.synchronize()
+    assert rel_l2(y.cpu().numpy(), o.vmult(x)) <= 1e-12
+    assert rel_l2(d.cpu().numpy(), o.diagonal()) <= 1e-12
