@@ -210,6 +210,18 @@ int fem_op_vmult_phase(fem_op* op, void* dst, const void* src, int32_t phase, vo
  * fem_op_params.kernel_variant); used by the autotuner.  No counterpart in
  * the reference (deal.II picks its vectorisation at compile time). */
 int fem_op_set_kernel_variant(fem_op* op, int32_t variant);
+/* ---- assembled-matrix comparison -----------------------------------------
+ * The reference compares its matrix-free vmult with a Trilinos sparse
+ * matrix-vector product on the same DoFs (CG/cells_batched/application.cc:
+ * 1944-1988).  fem_op_element_matrices writes the dense cell matrices of a
+ * FEM_CG operator to device memory [n_cells][K][K] (operator precision,
+ * unconstrained; the caller assembles them with fem_op_copy_dof_map and the
+ * constrained mask: constrained rows and columns dropped, ones on their
+ * diagonal).  fem_csr_spmv is y = A x for a device CSR matrix (row_ptr int64
+ * [n_rows + 1], col int32, val and vectors in `precision`). */
+int fem_op_element_matrices(fem_op* op, void* mats, void* stream);
+int fem_csr_spmv(int64_t n_rows, const int64_t* row_ptr, const int32_t* col, const void* val, const void* x,
+                 void* y, int32_t precision, void* stream);
 /* Algorithmic work of one vmult: flops and bytes of the fused kernels. */
 int fem_op_work(const fem_op* op, double* flops, double* bytes);
 /* Device-side status of the operator's kernels since the last call, then

@@ -189,6 +189,29 @@ int fem_op_create(fem_mesh* mesh, int32_t degree, int32_t kind, int32_t precisio
   });
 }
 
+int fem_op_element_matrices(fem_op* op, void* mats, void* stream) {
+  return guarded([&] {
+    REQUIRE_PTR(op);
+    REQUIRE_PTR(mats);
+    op->op->element_matrices(mats, static_cast<cudaStream_t>(stream));
+  });
+}
+
+int fem_csr_spmv(int64_t n_rows, const int64_t* row_ptr, const int32_t* col, const void* val, const void* x, void* y,
+                 int32_t precision, void* stream) {
+  return guarded([&] {
+    REQUIRE_PTR(row_ptr);
+    REQUIRE_PTR(col);
+    REQUIRE_PTR(val);
+    REQUIRE_PTR(x);
+    REQUIRE_PTR(y);
+    SFEM_REQUIRE(n_rows >= 0, FEM_ERR_ARG, "fem_csr_spmv: n_rows must be >= 0");
+    SFEM_REQUIRE(precision == FEM_FP64 || precision == FEM_FP32, FEM_ERR_ARG, "fem_csr_spmv: bad precision");
+    SFEM_REQUIRE(x != y, FEM_ERR_ARG, "fem_csr_spmv: x and y must not alias");
+    sfem::csr_spmv(n_rows, row_ptr, col, val, x, y, precision, static_cast<cudaStream_t>(stream));
+  });
+}
+
 int fem_op_destroy(fem_op* op) {
   return guarded([&] { delete op; });
 }

@@ -81,6 +81,49 @@ __global__ void __launch_bounds__(128, MINB) cg_cell_kernel(int64_t n_cells, con
     if (idx[i] >= 0) atomicAdd(dst + idx[i], y[i]);
 }
 
+// Dense element matrices of the cell operator, mats[c][r][i] = (A_K)_ri, one
+// thread per cell applying the local operator to each unit vector (set-up of
+// the assembled-matrix comparison; constraints are applied at assembly).
+template <int P, typename T>
+__global__ void __launch_bounds__(128) cg_element_matrix_kernel(int64_t n_cells, const T* __restrict__ geo,
+                                                                T* __restrict__ mats) {
+  using O = gen::Ops<P>;
+  constexpr int K = O::K;
+  const int64_t c = blockIdx.x * int64_t(blockDim.x) + threadIdx.x;
+  if (c >= n_cells) return;
+  T G[6];
+#pragma unroll
+  for (int k = 0; k < 6; ++k) G[k] = __ldg(geo + k * n_cells + c);
+  T* m = mats + c * K * K;
+  for (int i = 0; i < K; ++i) {
+    T u[K], y[K];
+#pragma unroll
+    for (int j = 0; j < K; ++j) u[j] = j == i ? T(1) : T(0);
+    cg_local_apply<P>(G, u, y);
+#pragma unroll
+    for (int r = 0; r < K; ++r) m[r * K + i] = y[r];
+  }
+}
+
+// y = A x for a CSR matrix, LANES threads per row (partial sums reduced with
+// warp shuffles); the assembled-matrix baseline of the matrix-free vmult.
+template <typename T, int LANES>
+__global__ void __launch_bounds__(256) csr_spmv_kernel(int64_t n_rows, const int64_t* __restrict__ row_ptr,
+                                                       const int32_t* __restrict__ col, const T* __restrict__ val,
+                                                       const T* __restrict__ x, T* __restrict__ y) {
+  const int64_t t = blockIdx.x * int64_t(blockDim.x) + threadIdx.x;
+  const int64_t row = t / LANES;
+  const int lane = int(t % LANES);
+  T s = T(0);
+  if (row < n_rows) {
+    const int64_t b = __ldg(row_ptr + row), e = __ldg(row_ptr + row + 1);
+    for (int64_t k = b + lane; k < e; k += LANES) s += __ldg(val + k) * __ldg(x + __ldg(col + k));
+  }
+#pragma unroll
+  for (int o = LANES / 2; o > 0; o >>= 1) s += __shfl_down_sync(0xffffffffu, s, o, LANES);
+  if (row < n_rows && lane == 0) y[row] = s;
+}
+
 // Macro-element form for Kuhn meshes: one thread per hex, i.e. the 6
 // consecutive tets that subdivide it.  The 6 tets share most of their DoFs
 // (P1: 8 distinct of 24, P2: 27 of 60, P3: 64 of 120), so the thread gathers

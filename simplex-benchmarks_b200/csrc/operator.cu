@@ -753,6 +753,17 @@ class CGOperator final : public Operator {
 
   const int32_t* device_dof_table() const override { return d_dofs.p; }
 
+  void element_matrices(void* out, cudaStream_t s) override {
+    T* m = static_cast<T*>(out);
+    const unsigned grid = blocks_for(std::max<int64_t>(n_cells, 1), 128);
+    switch (cfg.degree) {
+      case 1: cg_element_matrix_kernel<1, T><<<grid, 128, 0, s>>>(n_cells, d_geo.p, m); break;
+      case 2: cg_element_matrix_kernel<2, T><<<grid, 128, 0, s>>>(n_cells, d_geo.p, m); break;
+      case 3: cg_element_matrix_kernel<3, T><<<grid, 128, 0, s>>>(n_cells, d_geo.p, m); break;
+    }
+    SFEM_CUDA(cudaGetLastError());
+  }
+
   void work(double& flops, double& bytes) const override {
     const int p = cfg.degree, kq = kq_of(p);
     const double per_cell = 2.0 * (2 * nnz_grad_rt(p) + 9 * kq + 3 * kq * kq);
@@ -1176,6 +1187,19 @@ std::unique_ptr<Operator> make_operator(const Mesh& mesh, const OpConfig& cfg) {
   }
   op->mesh = &mesh;
   return op;
+}
+
+void csr_spmv(int64_t n_rows, const int64_t* row_ptr, const int32_t* col, const void* val, const void* x, void* y,
+              int precision, cudaStream_t s) {
+  constexpr int LANES = 8;
+  const unsigned grid = blocks_for(std::max<int64_t>(n_rows, 1) * LANES, 256);
+  if (precision == FEM_FP64)
+    csr_spmv_kernel<double, LANES><<<grid, 256, 0, s>>>(n_rows, row_ptr, col, static_cast<const double*>(val),
+                                                        static_cast<const double*>(x), static_cast<double*>(y));
+  else
+    csr_spmv_kernel<float, LANES><<<grid, 256, 0, s>>>(n_rows, row_ptr, col, static_cast<const float*>(val),
+                                                       static_cast<const float*>(x), static_cast<float*>(y));
+  SFEM_CUDA(cudaGetLastError());
 }
 
 std::unique_ptr<Operator> make_local_operator(std::shared_ptr<const Mesh> mesh, const CGDofs* dofs,

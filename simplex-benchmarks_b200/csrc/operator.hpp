@@ -96,6 +96,10 @@ class Operator {
     throw Error(FEM_ERR_ARG, "this operator kind uses no scratch memory");
   }
   void inverse_diagonal(void* diag, cudaStream_t s);
+  // CG: dense element matrices of the cell operator, device [n_cells][K][K]
+  virtual void element_matrices(void* out, cudaStream_t s) {
+    throw Error(FEM_ERR_ARG, "element matrices: CG operators only");
+  }
   // device-side status bits of the operator's kernels since the last call
   // (bit 0: a tensor-core kernel gave up on a bounded wait); clear resets them
   virtual int status(bool clear) { return 0; }
@@ -141,5 +145,9 @@ class Batch {
   virtual void set_variant(int v) = 0;
 };
 std::unique_ptr<Batch> make_batch(const std::vector<Operator*>& ops);
+
+// y = A x for a CSR matrix on the device (row_ptr int64, col int32)
+void csr_spmv(int64_t n_rows, const int64_t* row_ptr, const int32_t* col, const void* val, const void* x, void* y,
+              int precision, cudaStream_t s);
 
 }  // namespace sfem

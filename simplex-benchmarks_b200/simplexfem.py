@@ -96,6 +96,9 @@ _PROTOS = [
     ("fem_op_create", C.c_int, [C.c_void_p, C.c_int32, C.c_int32, C.c_int32, C.POINTER(OpParams),
                                 C.POINTER(C.c_void_p)]),
     ("fem_op_destroy", C.c_int, [C.c_void_p]),
+    ("fem_op_element_matrices", C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p]),
+    ("fem_csr_spmv", C.c_int, [C.c_int64, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_int32,
+                               C.c_void_p]),
     ("fem_op_m", C.c_int, [C.c_void_p, C.POINTER(C.c_uint64)]),
     ("fem_op_info", C.c_int, [C.c_void_p, C.POINTER(C.c_int32), C.POINTER(C.c_int32), C.POINTER(C.c_int32),
                               C.POINTER(C.c_int32), C.POINTER(C.c_int64), C.POINTER(C.c_int32)]),
@@ -409,6 +412,43 @@ class Operator:
         if getattr(self, "handle", None) and _lib is not None:
             _lib.fem_op_destroy(self.handle)
             self.handle = None
+
+
+class CSRMatrix:
+    """The CG operator assembled into a device CSR matrix (the reference's
+    Trilinos SparseMatrix comparison, CG/cells_batched/application.cc:1944-1988):
+    the cell matrices come from fem_op_element_matrices, constrained rows and
+    columns are dropped and get a one on the diagonal (the operator's
+    identity rows); vmult runs fem_csr_spmv."""
+
+    def __init__(self, op):
+        import torch
+        if op.kind != FEM_CG:
+            raise FemError(FEM_ERR_ARG, "CSRMatrix: CG operators only")
+        K, n = op.dofs_per_cell, op.n_cells
+        mats = torch.empty((n, K, K), dtype=op.dtype, device="cuda")
+        check(lib().fem_op_element_matrices(op.handle, _ptr(mats), _stream_ptr(None)))
+        dofs = torch.from_numpy(op.dof_map().astype(np.int64)).cuda()  # [n][K]
+        free = ~torch.from_numpy(op.constrained().astype(bool)).cuda()
+        rows = dofs[:, :, None].expand(n, K, K).reshape(-1)
+        cols = dofs[:, None, :].expand(n, K, K).reshape(-1)
+        vals = mats.reshape(-1)
+        keep = free[rows] & free[cols]
+        cidx = torch.nonzero(~free).reshape(-1)
+        rows = torch.cat([rows[keep], cidx])
+        cols = torch.cat([cols[keep], cidx])
+        vals = torch.cat([vals[keep], torch.ones(len(cidx), dtype=op.dtype, device="cuda")])
+        del mats, keep
+        m = op.m()
+        A = torch.sparse_coo_tensor(torch.stack([rows, cols]), vals, (m, m)).coalesce().to_sparse_csr()
+        self.row_ptr = A.crow_indices().to(torch.int64).contiguous()
+        self.col = A.col_indices().to(torch.int32).contiguous()
+        self.val = A.values().contiguous()
+        self.m, self.nnz, self.precision = m, int(self.val.numel()), op.precision
+
+    def vmult(self, dst, src, stream=None):
+        check(lib().fem_csr_spmv(self.m, _ptr(self.row_ptr), _ptr(self.col), _ptr(self.val), _ptr(src), _ptr(dst),
+                                 self.precision, _stream_ptr(stream)))
 
 
 class Partition:
