@@ -158,6 +158,8 @@ OpConfig op_config(int32_t degree, int32_t kind, int32_t precision, const fem_op
       if (kind == FEM_HELMHOLTZ) {
         cfg.mass = params->mass_coefficient;
         cfg.n_components = params->n_components > 0 ? params->n_components : 3;
+      } else if (kind == FEM_CG) {
+        cfg.n_components = params->n_components > 0 ? params->n_components : 1;
       }
       cfg.penalty = params->penalty;
       cfg.kernel_variant = params->kernel_variant;

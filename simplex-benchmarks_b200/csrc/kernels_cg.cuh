@@ -81,6 +81,52 @@ __global__ void __launch_bounds__(128, MINB) cg_cell_kernel(int64_t n_cells, con
     if (idx[i] >= 0) atomicAdd(dst + idx[i], y[i]);
 }
 
+// Vector Laplacian with NC interleaved components (global index NC g + comp
+// of node DoF g), the optimized kernels of the reference's components-batched
+// CG operator (CG/components_batched/application.cc:1025-1216: the scalar
+// metric applied to every component).  One thread per cell: the node table
+// is read once and the cell's NC K values gathered, every component runs the
+// fused local operator, results added atomically.  constrained lists vector
+// indices (rows dst = src).
+template <int P, typename T, int NC>
+__global__ void __launch_bounds__(128) cg_cell_vec_kernel(int64_t n_cells, const int32_t* __restrict__ dofs,
+                                                          const T* __restrict__ geo, const T* __restrict__ src,
+                                                          T* __restrict__ dst, int64_t n_constrained,
+                                                          const int32_t* __restrict__ constrained) {
+  using O = gen::Ops<P>;
+  const int64_t c = blockIdx.x * int64_t(blockDim.x) + threadIdx.x;
+  if (c < n_constrained) {
+    const int32_t i = constrained[c];
+    dst[i] = src[i];
+  }
+  if (c >= n_cells) return;
+  int32_t idx[O::K];
+#pragma unroll
+  for (int i = 0; i < O::K; ++i) idx[i] = __ldg(dofs + i * n_cells + c);
+  T G[6];
+#pragma unroll
+  for (int k = 0; k < 6; ++k) G[k] = __ldg(geo + k * n_cells + c);
+#pragma unroll 1
+  for (int comp = 0; comp < NC; ++comp) {
+    T u[O::K], y[O::K];
+#pragma unroll
+    for (int i = 0; i < O::K; ++i) u[i] = idx[i] >= 0 ? __ldg(src + int64_t(NC) * idx[i] + comp) : T(0);
+    cg_local_apply<P>(G, u, y);
+#pragma unroll
+    for (int i = 0; i < O::K; ++i)
+      if (idx[i] >= 0) atomicAdd(dst + int64_t(NC) * idx[i] + comp, y[i]);
+  }
+}
+
+// the scalar diagonal d (node DoFs) repeated on every component
+template <typename T, int NC>
+__global__ void expand_components(int64_t n, const T* __restrict__ d, T* __restrict__ out) {
+  const int64_t i = blockIdx.x * int64_t(blockDim.x) + threadIdx.x;
+  if (i >= n) return;
+#pragma unroll
+  for (int comp = 0; comp < NC; ++comp) out[NC * i + comp] = d[i];
+}
+
 // Dense element matrices of the cell operator, mats[c][r][i] = (A_K)_ri, one
 // thread per cell applying the local operator to each unit vector (set-up of
 // the assembled-matrix comparison; constraints are applied at assembly).

@@ -471,8 +471,8 @@ class MultigridImpl final : public Multigrid {
 
   MultigridImpl(const Operator& fine, const MGParams& prm) {
     params = prm;
-    SFEM_REQUIRE((fine.cfg.kind == FEM_CG || fine.cfg.kind == FEM_DG) && fine.mesh, FEM_ERR_ARG,
-                 "multigrid: fine operator must be CG or DG (one component)");
+    SFEM_REQUIRE((fine.cfg.kind == FEM_CG || fine.cfg.kind == FEM_DG) && fine.cfg.n_components == 1 && fine.mesh,
+                 FEM_ERR_ARG, "multigrid: fine operator must be CG or DG (one component)");
     SFEM_REQUIRE(prm.c_transfer == 0 || prm.c_transfer == 1, FEM_ERR_ARG, "multigrid: c_transfer must be 0 or 1");
     SFEM_REQUIRE(prm.smoother_degree >= 1 && prm.smoother_degree <= 32, FEM_ERR_ARG, "multigrid: smoother degree");
     const Mesh& mf = *fine.mesh;

@@ -773,6 +773,116 @@ class CGOperator final : public Operator {
   }
 };
 
+// ------------------------------------------------------- CG, 3 components --
+// Vector Laplacian with the components of every node DoF interleaved
+// (index 3 g + comp), as the reference's components-batched CG operator
+// (CG/components_batched/application.cc:778-1611, FESystem of dim
+// FE_SimplexP).  Homogeneous Dirichlet on every component of the boundary
+// nodes.  Cell kernel only.
+template <typename T>
+class CGVectorOperator final : public Operator {
+ public:
+  static constexpr int NC = 3;
+  DevBuf<int32_t> d_dofs;         // [K][n_cells] node DoFs, -1 = constrained
+  DevBuf<T> d_geo;                // [6][n_cells]
+  DevBuf<int32_t> d_constrained;  // constrained vector indices
+  int64_t n_nodes = 0;
+  std::vector<int32_t> node_dofs;  // [n_cells][K]
+
+  CGVectorOperator(const Mesh& mesh, const OpConfig& c) {
+    cfg = c;
+    const CGDofs dofs = build_cg_dofs(mesh, cfg.degree);
+    K = dofs.K;
+    n_cells = mesh.n_cells;
+    n_nodes = dofs.n_dofs;
+    m = NC * n_nodes;
+    n_interior_faces = mesh.n_interior_faces;
+    n_boundary_faces = mesh.n_boundary_faces;
+    node_dofs = dofs.cell_dofs;
+    cell_dofs.resize(size_t(NC) * K * n_cells);
+    for (int64_t cc = 0; cc < n_cells; ++cc)
+      for (int comp = 0; comp < NC; ++comp)
+        for (int i = 0; i < K; ++i)
+          cell_dofs[(cc * NC + comp) * K + i] = NC * dofs.cell_dofs[K * cc + i] + comp;
+    constrained.assign(m, 0);
+    std::vector<int32_t> cl;
+    for (int64_t g = 0; g < n_nodes; ++g)
+      if (dofs.constrained[g])
+        for (int comp = 0; comp < NC; ++comp) {
+          constrained[NC * g + comp] = 1;
+          cl.push_back(int32_t(NC * g + comp));
+        }
+    support = dofs.support;
+    std::vector<int32_t> idx(size_t(K) * n_cells);
+    for (int64_t cc = 0; cc < n_cells; ++cc)
+      for (int i = 0; i < K; ++i) {
+        const int32_t g = dofs.cell_dofs[K * cc + i];
+        idx[size_t(i) * n_cells + cc] = dofs.constrained[g] ? -1 : g;
+      }
+    d_dofs.upload(idx);
+    std::vector<T> geo(6 * size_t(n_cells));
+    for (int64_t cc = 0; cc < n_cells; ++cc) {
+      double G[6];
+      metric(cell_geometry(mesh, cc), G);
+      for (int k = 0; k < 6; ++k) geo[size_t(k) * n_cells + cc] = T(G[k]);
+    }
+    d_geo.upload(geo);
+    d_constrained.upload(cl);
+  }
+
+  void vmult(void* dst, const void* src, cudaStream_t s) override {
+    vmult_phase(dst, src, 1, s);
+    vmult_phase(dst, src, 2, s);
+  }
+
+  void vmult_phase(void* dst, const void* src, int phase, cudaStream_t s) override {
+    T* d = static_cast<T*>(dst);
+    const T* x = static_cast<const T*>(src);
+    if (phase == 1) {
+      SFEM_CUDA(cudaMemsetAsync(d, 0, sizeof(T) * m, s));
+      return;
+    }
+    const unsigned grid = blocks_for(std::max<int64_t>(n_cells, int64_t(d_constrained.n)), 128);
+    switch (cfg.degree) {
+      case 1: cg_cell_vec_kernel<1, T, NC><<<grid, 128, 0, s>>>(n_cells, d_dofs.p, d_geo.p, x, d, d_constrained.n, d_constrained.p); break;
+      case 2: cg_cell_vec_kernel<2, T, NC><<<grid, 128, 0, s>>>(n_cells, d_dofs.p, d_geo.p, x, d, d_constrained.n, d_constrained.p); break;
+      case 3: cg_cell_vec_kernel<3, T, NC><<<grid, 128, 0, s>>>(n_cells, d_dofs.p, d_geo.p, x, d, d_constrained.n, d_constrained.p); break;
+    }
+    SFEM_CUDA(cudaGetLastError());
+  }
+
+  void diagonal(void* diag, cudaStream_t s) override {
+    DevBuf<T> dn(n_nodes);
+    SFEM_CUDA(cudaMemsetAsync(dn.p, 0, sizeof(T) * n_nodes, s));
+    std::vector<int32_t> cn;
+    for (int64_t g = 0; g < n_nodes; ++g)
+      if (constrained[NC * g]) cn.push_back(int32_t(g));
+    DevBuf<int32_t> d_cn;
+    d_cn.upload(cn);
+    const unsigned grid = blocks_for(std::max<int64_t>(n_cells, int64_t(cn.size())), 128);
+    switch (cfg.degree) {
+      case 1: cg_diagonal_kernel<1, T><<<grid, 128, 0, s>>>(n_cells, d_dofs.p, d_geo.p, dn.p, d_cn.n, d_cn.p); break;
+      case 2: cg_diagonal_kernel<2, T><<<grid, 128, 0, s>>>(n_cells, d_dofs.p, d_geo.p, dn.p, d_cn.n, d_cn.p); break;
+      case 3: cg_diagonal_kernel<3, T><<<grid, 128, 0, s>>>(n_cells, d_dofs.p, d_geo.p, dn.p, d_cn.n, d_cn.p); break;
+    }
+    expand_components<T, NC><<<blocks_for(std::max<int64_t>(n_nodes, 1), 256), 256, 0, s>>>(
+        n_nodes, dn.p, static_cast<T*>(diag));
+    SFEM_CUDA(cudaGetLastError());
+    SFEM_CUDA(cudaStreamSynchronize(s));  // the temporaries are freed on return
+  }
+
+  void rhs(const RhsDesc& rd, void* dst, cudaStream_t s) override {
+    throw Error(FEM_ERR_ARG, "rhs: not provided for the 3-component CG operator");
+  }
+
+  void work(double& flops, double& bytes) const override {
+    const int p = cfg.degree, kq = kq_of(p);
+    flops = NC * 2.0 * (2 * nnz_grad_rt(p) + 9 * kq + 3 * kq * kq) * double(n_cells);
+    const double sz = double(sizeof(T));
+    bytes = 2 * sz * double(m) + 4.0 * K * double(n_cells) + 6 * sz * double(n_cells);
+  }
+};
+
 // ------------------------------------------------------------------ DG ----
 template <typename T>
 class DGOperator final : public Operator {
@@ -1176,9 +1286,17 @@ std::unique_ptr<Operator> make_operator(const Mesh& mesh, const OpConfig& cfg) {
   SFEM_REQUIRE(cfg.precision == FEM_FP64 || cfg.precision == FEM_FP32, FEM_ERR_ARG, "operator: bad precision");
   std::unique_ptr<Operator> op;
   if (cfg.kind == FEM_CG) {
-    SFEM_REQUIRE(cfg.n_components == 1, FEM_ERR_ARG, "CG: n_components must be 1");
-    if (cfg.precision == FEM_FP64) op = std::make_unique<CGOperator<double>>(mesh, cfg);
-    else op = std::make_unique<CGOperator<float>>(mesh, cfg);
+    SFEM_REQUIRE(cfg.n_components == 1 || cfg.n_components == 3, FEM_ERR_ARG, "CG: n_components must be 1 or 3");
+    if (cfg.n_components == 3) {
+      SFEM_REQUIRE(!cfg.weak_bc && (cfg.kernel_variant == 0 || cfg.kernel_variant == 1), FEM_ERR_ARG,
+                   "CG with 3 components: strong constraints and the cell kernel only");
+      if (cfg.precision == FEM_FP64) op = std::make_unique<CGVectorOperator<double>>(mesh, cfg);
+      else op = std::make_unique<CGVectorOperator<float>>(mesh, cfg);
+    } else if (cfg.precision == FEM_FP64) {
+      op = std::make_unique<CGOperator<double>>(mesh, cfg);
+    } else {
+      op = std::make_unique<CGOperator<float>>(mesh, cfg);
+    }
   } else if (cfg.kind == FEM_DG || cfg.kind == FEM_HELMHOLTZ) {
     if (cfg.precision == FEM_FP64) op = std::make_unique<DGOperator<double>>(mesh, cfg);
     else op = std::make_unique<DGOperator<float>>(mesh, cfg);

@@ -358,3 +358,33 @@ def test_dg_vmult_on_unaligned_views(cuda, kind, p, precision):
     op.vmult(by[1:], bx[1:])
     torch.cuda.synchronize()
     assert torch.equal(by[1:], y)
+
+
+@pytest.mark.parametrize("precision", ["fp64", "fp32"])
+@pytest.mark.parametrize("p", [1, 2, 3])
+def test_cg_three_component_operator(cuda, p, precision):
+    """CG vector Laplacian with 3 interleaved components (the reference's
+    components-batched CG operator, CG/components_batched/application.cc:
+    1025-1216): every component equals the scalar oracle on that component's
+    values; constrained rows are identity rows; the diagonal repeats the
+    scalar one."""
+    import torch
+    mesh = sf.Mesh((5, 4, 6), jitter=0.1, seed=12)
+    op = sf.Operator(mesh, p, "cg", precision, n_components=3)
+    o = orc.for_mesh(mesh, p, orc.CG)
+    assert op.m() == 3 * o.n and op.n_components == 3
+    x = seeded_src(op.m(), 13)
+    y = run_product(op, x)
+    xr = oracle_input(op, x)
+    for comp in range(3):
+        assert rel_l2(y[comp::3], o.vmult(xr[comp::3])) <= TOL[precision], comp
+    cm = op.constrained().astype(bool)
+    assert cm.sum() == 3 * o.constrained.sum()
+    d = op.initialize_dof_vector()
+    op.compute_diagonal(d)
+    torch.cuda.synchronize()
+    dd = d.double().cpu().numpy()
+    for comp in range(3):
+        assert rel_l2(dd[comp::3], o.diagonal()) <= TOL[precision]
+    with pytest.raises(sf.FemError):
+        sf.Multigrid(op)
