@@ -126,6 +126,20 @@ int fem_mesh_create_from_arrays(int64_t n_vertices, const double* xyz /* [n_vert
                                 const int32_t* cell_vertices /* [n_cells][4] */, int32_t reorder, fem_mesh** out);
 /* The same from a legacy ASCII VTK unstructured grid of tetrahedra (VTK cell type 10). */
 int fem_mesh_read_vtk(const char* path, int32_t reorder, fem_mesh** out);
+/* Curvilinear geometry (the reference's non-affine cells, MappingFE on a
+ * manifold: CG/cells_batched/application.cc:1361-1376,
+ * DG/components_batched/application.cc:1547): every point x of the mesh's
+ * bounding box moves to x + amplitude * prod_d sin(pi xi_d) * (hi - lo), xi in
+ * [0,1]^3 the box coordinates (the box boundary stays), and every cell gets a
+ * quadratic geometry (its moved vertices and moved edge midpoints).  FEM_CG
+ * operators on a curved mesh apply a per-quadrature-point metric (collapsed
+ * Gauss-Legendre rule, p + 1 points per direction); DG / Helmholtz operators,
+ * partitions and multigrid need affine meshes.  |amplitude| < 0.5; an
+ * amplitude that inverts a cell is FEM_ERR_ARG. */
+int fem_mesh_curve(fem_mesh* mesh, double amplitude);
+/* edge geometry nodes of a curved mesh, [n_cells][6][3] in the edge order
+ * (0,1),(0,2),(0,3),(1,2),(1,3),(2,3) of the sorted cell vertices */
+int fem_mesh_copy_edge_nodes(const fem_mesh* mesh, double* xyz);
 /* input index of every cell of a mesh from arrays (identity for Kuhn meshes) */
 int fem_mesh_copy_input_cells(const fem_mesh* mesh, int64_t* input_cell /* [n_cells] */);
 int fem_mesh_destroy(fem_mesh* mesh);

@@ -50,6 +50,10 @@ struct oracle_ctx {
   double qc_w[MAXQ * MAXQ * MAXQ];
   double qc_phi[MAXQ * MAXQ * MAXQ][MAXK];
   double qc_dphi[MAXQ * MAXQ * MAXQ][MAXK][3];
+  double qc_xi[MAXQ * MAXQ * MAXQ][3];
+  /* curved cells: P2 geometry (edge nodes [nc][6][3]) and its gradients at the cell points */
+  double* edge;
+  double qc_gdphi[MAXQ * MAXQ * MAXQ][10][3];
   /* face quadrature (reference triangle s,t) */
   int nqf;
   double qf_st[MAXQ * MAXQ][2];
@@ -208,6 +212,9 @@ static void build_quadrature(oracle_ctx* ctx) {
       for (int c = 0; c < n; ++c) {
         const double u = t[a], v = t[b], s = t[c];
         double xi[3] = {u, v * (1 - u), s * (1 - u) * (1 - v)};
+        ctx->qc_xi[q][0] = xi[0];
+        ctx->qc_xi[q][1] = xi[1];
+        ctx->qc_xi[q][2] = xi[2];
         ctx->qc_w[q] = w[a] * w[b] * w[c] * (1 - u) * (1 - u) * (1 - v);
         eval_basis(&ctx->B, xi, ctx->qc_phi[q], ctx->qc_dphi[q]);
         ++q;
@@ -224,6 +231,18 @@ static void build_quadrature(oracle_ctx* ctx) {
   ctx->nqf = q;
 }
 
+int oracle_set_p2_geometry(oracle_ctx* ctx, const double* edge_nodes) {
+  if (!ctx || !edge_nodes || ctx->prm.kind != ORACLE_CG) return -1;
+  basis_t G2;
+  if (build_basis(2, &G2)) return -3;
+  free(ctx->edge);
+  ctx->edge = (double*)malloc(sizeof(double) * 18 * ctx->nc);
+  if (!ctx->edge) return -2;
+  memcpy(ctx->edge, edge_nodes, sizeof(double) * 18 * ctx->nc);
+  for (int q = 0; q < ctx->nqc; ++q) eval_basis(&G2, ctx->qc_xi[q], NULL, ctx->qc_gdphi[q]);
+  return 0;
+}
+
 int oracle_quadrature_sizes(const oracle_ctx* ctx, int32_t* nc, int32_t* nf) {
   if (nc) *nc = ctx->nqc;
   if (nf) *nf = ctx->nqf;
@@ -231,6 +250,14 @@ int oracle_quadrature_sizes(const oracle_ctx* ctx, int32_t* nc, int32_t* nf) {
 }
 
 /* --------------------------------------------------------------- geometry -- */
+static void invert_jacobian(geom_t* g);
+
+static void set_jacobian(geom_t* g, const double J[3][3]) {
+  for (int i = 0; i < 3; ++i)
+    for (int j = 0; j < 3; ++j) g->J[i][j] = J[i][j];
+  invert_jacobian(g);
+}
+
 static void make_geom(const double* x, const int32_t* cv, geom_t* g) {
   const double* x0 = x + 3 * (int64_t)cv[0];
   for (int d = 0; d < 3; ++d) g->x0[d] = x0[d];
@@ -238,6 +265,10 @@ static void make_geom(const double* x, const int32_t* cv, geom_t* g) {
     const double* xj = x + 3 * (int64_t)cv[j + 1];
     for (int i = 0; i < 3; ++i) g->J[i][j] = xj[i] - x0[i];
   }
+  invert_jacobian(g);
+}
+
+static void invert_jacobian(geom_t* g) {
   double(*J)[3] = g->J;
   double c00 = J[1][1] * J[2][2] - J[1][2] * J[2][1];
   double c01 = J[1][2] * J[2][0] - J[1][0] * J[2][2];
@@ -401,6 +432,7 @@ void oracle_destroy(oracle_ctx* ctx) {
   free(ctx->nbf);
   free(ctx->geo);
   free(ctx->tau);
+  free(ctx->edge);
   free(ctx->ih);
   free(ctx);
 }
@@ -420,9 +452,24 @@ static void cell_apply(const oracle_ctx* ctx, int64_t c, const double* u /* [nc]
   memset(y, 0, sizeof(double) * K * NC);
   /* cell term */
   for (int q = 0; q < ctx->nqc; ++q) {
-    const double W = ctx->qc_w[q] * adet;
+    double W = ctx->qc_w[q] * adet;
     double gphi[MAXK][3];
-    for (int i = 0; i < K; ++i) push_grad(g, ctx->qc_dphi[q][i], gphi[i]);
+    if (ctx->edge) {
+      /* curved cell: Jacobian of the quadratic geometry at this point */
+      geom_t gq;
+      const double* X[10];
+      for (int v = 0; v < 4; ++v) X[v] = ctx->x + 3 * (int64_t)ctx->cells[4 * c + v];
+      for (int e = 0; e < 6; ++e) X[4 + e] = ctx->edge + 18 * c + 3 * e;
+      double J[3][3] = {{0}};
+      for (int k = 0; k < 10; ++k)
+        for (int i = 0; i < 3; ++i)
+          for (int j = 0; j < 3; ++j) J[i][j] += X[k][i] * ctx->qc_gdphi[q][k][j];
+      set_jacobian(&gq, J);
+      W = ctx->qc_w[q] * fabs(gq.det);
+      for (int i = 0; i < K; ++i) push_grad(&gq, ctx->qc_dphi[q][i], gphi[i]);
+    } else {
+      for (int i = 0; i < K; ++i) push_grad(g, ctx->qc_dphi[q][i], gphi[i]);
+    }
     for (int comp = 0; comp < NC; ++comp) {
       const double* uc = u + comp * K;
       double gu[3] = {0, 0, 0}, val = 0;

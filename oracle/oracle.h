@@ -86,6 +86,11 @@ int oracle_kuhn_mesh(const int32_t n[3], const double lo[3], const double hi[3],
  * NULL only counts.  cell_dofs [n_cells][k], constrained [n_dofs]. */
 int64_t oracle_cg_numbering(int64_t n_vertices, int64_t n_cells, const int32_t* cells, const int32_t* nb,
                             int32_t degree, int32_t* cell_dofs, uint8_t* constrained);
+/* CG on curved cells: quadratic geometry from the cells' vertices and their
+ * edge nodes [n_cells][6][3] (edges (0,1),(0,2),(0,3),(1,2),(1,3),(2,3));
+ * the cell integrals then use the Jacobian at every quadrature point
+ * (CG/cells_batched/application.cc:1361-1376). */
+int oracle_set_p2_geometry(oracle_ctx* ctx, const double* edge_nodes);
 /* quadrature sizes actually used */
 int oracle_quadrature_sizes(const oracle_ctx* ctx, int32_t* n_cell_points, int32_t* n_face_points);
 

@@ -47,6 +47,8 @@ def lib():
         L.oracle_n_dofs.restype = C.c_int64
         L.oracle_n_dofs.argtypes = [C.c_void_p]
         L.oracle_quadrature_sizes.argtypes = [C.c_void_p, C.POINTER(C.c_int32), C.POINTER(C.c_int32)]
+        L.oracle_set_p2_geometry.restype = C.c_int
+        L.oracle_set_p2_geometry.argtypes = [C.c_void_p, C.c_void_p]
         L.oracle_kuhn_mesh.restype = C.c_int
         L.oracle_kuhn_mesh.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_double, C.c_uint64, C.c_void_p,
                                        C.c_void_p, C.c_void_p, C.c_void_p]
@@ -82,6 +84,12 @@ class Oracle:
         self.n = lib().oracle_n_dofs(h)
         self.K = (degree + 1) * (degree + 2) * (degree + 3) // 6
         self.nc = n_components
+
+    def set_p2_geometry(self, edge_nodes):
+        """CG on curved cells: quadratic geometry from the edge nodes [n_cells][6][3]."""
+        self._edge = np.ascontiguousarray(edge_nodes, np.float64)
+        if lib().oracle_set_p2_geometry(self.h, self._edge.ctypes.data) != 0:
+            raise RuntimeError("oracle_set_p2_geometry failed")
 
     def vmult(self, src):
         src = np.ascontiguousarray(src, np.float64)

@@ -76,6 +76,22 @@ int fem_mesh_read_vtk(const char* path, int32_t reorder, fem_mesh** out) {
   });
 }
 
+int fem_mesh_curve(fem_mesh* mesh, double amplitude) {
+  return guarded([&] {
+    REQUIRE_PTR(mesh);
+    sfem::curve_mesh(mesh->mesh, amplitude);
+  });
+}
+
+int fem_mesh_copy_edge_nodes(const fem_mesh* mesh, double* xyz) {
+  return guarded([&] {
+    REQUIRE_PTR(mesh);
+    REQUIRE_PTR(xyz);
+    SFEM_REQUIRE(mesh->mesh.curved, FEM_ERR_STATE, "fem_mesh_copy_edge_nodes: the mesh is not curved");
+    std::memcpy(xyz, mesh->mesh.edge_x.data(), mesh->mesh.edge_x.size() * sizeof(double));
+  });
+}
+
 int fem_mesh_copy_input_cells(const fem_mesh* mesh, int64_t* input_cell) {
   return guarded([&] {
     REQUIRE_PTR(mesh);

@@ -233,6 +233,43 @@ Mesh build_mesh_from_arrays(int64_t n_vertices, const double* x, int64_t n_cells
   return m;
 }
 
+void curve_mesh(Mesh& m, double amplitude) {
+  SFEM_REQUIRE(!m.curved, FEM_ERR_STATE, "curve: the mesh is already curved");
+  SFEM_REQUIRE(std::isfinite(amplitude) && std::fabs(amplitude) < 0.5, FEM_ERR_ARG,
+               "curve: |amplitude| must be below 0.5");
+  double lo[3] = {1e300, 1e300, 1e300}, hi[3] = {-1e300, -1e300, -1e300};
+  for (int64_t v = 0; v < m.n_vertices; ++v)
+    for (int a = 0; a < 3; ++a) {
+      lo[a] = std::min(lo[a], m.x[3 * v + a]);
+      hi[a] = std::max(hi[a], m.x[3 * v + a]);
+    }
+  auto phi = [&](const double* x, double* out) {
+    double s = amplitude;
+    for (int a = 0; a < 3; ++a) s *= std::sin(M_PI * (x[a] - lo[a]) / (hi[a] - lo[a]));
+    for (int a = 0; a < 3; ++a) out[a] = x[a] + s * (hi[a] - lo[a]);
+  };
+  std::vector<double> sign(m.n_cells);
+  for (int64_t c = 0; c < m.n_cells; ++c) sign[c] = cell_geometry(m, c).det > 0 ? 1.0 : -1.0;
+  m.edge_x.resize(18 * size_t(m.n_cells));
+  for (int64_t c = 0; c < m.n_cells; ++c)
+    for (int e = 0; e < 6; ++e) {
+      double mid[3];
+      for (int a = 0; a < 3; ++a)
+        mid[a] = 0.5 * (m.x[3 * int64_t(m.cell_vertices[4 * c + kEdges[e][0]]) + a] +
+                        m.x[3 * int64_t(m.cell_vertices[4 * c + kEdges[e][1]]) + a]);
+      phi(mid, &m.edge_x[18 * c + 3 * e]);
+    }
+  std::vector<double> moved(m.x.size());
+  for (int64_t v = 0; v < m.n_vertices; ++v) phi(&m.x[3 * v], &moved[3 * v]);
+  m.x.swap(moved);
+  for (int64_t c = 0; c < m.n_cells; ++c) {
+    const double det = cell_geometry(m, c).det;
+    SFEM_REQUIRE(det * sign[c] > 0, FEM_ERR_ARG, "curve: the amplitude inverts cell " + std::to_string(c));
+  }
+  m.curved = true;
+  m.structured = false;  // the h-levels of the multigrid are affine Kuhn meshes
+}
+
 Mesh read_vtk_mesh(const std::string& path, int reorder) {
   std::ifstream in(path);
   SFEM_REQUIRE(in.good(), FEM_ERR_ARG, "vtk: cannot open " + path);

@@ -46,6 +46,8 @@ struct Mesh {
   int64_t n_interior_faces = 0;
   int64_t n_boundary_faces = 0;
   bool structured = false;          // a Kuhn box (hex / cube kernels, h-multigrid)
+  bool curved = false;              // quadratic geometry: edge_x holds the edge nodes
+  std::vector<double> edge_x;       // [n_cells][6][3] geometry nodes of edges (0,1),(0,2),(0,3),(1,2),(1,3),(2,3)
   std::vector<int64_t> input_cell;  // meshes from arrays: input index of every cell
 
   // lexicographic vertex index of lattice point (i,j,k)
@@ -59,6 +61,13 @@ struct Mesh {
 };
 
 Mesh build_kuhn_mesh(const MeshDescription& d);
+
+// Curvilinear geometry: every point x of the mesh's bounding box moves to
+// x + amplitude * prod_d sin(pi xi_d) * (hi - lo), xi the box coordinates in
+// [0,1]^3 (the box boundary stays), and every cell gets a quadratic
+// (P2) geometry: its moved vertices and the moved midpoints of its straight
+// edges.  Cells whose orientation would flip are rejected.
+void curve_mesh(Mesh& m, double amplitude);
 
 // Face neighbours (nb, nbf) and face counts of a mesh with sorted cell vertices.
 void build_face_adjacency(Mesh& m);

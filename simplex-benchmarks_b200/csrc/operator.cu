@@ -1285,7 +1285,11 @@ std::unique_ptr<Operator> make_operator(const Mesh& mesh, const OpConfig& cfg) {
   SFEM_REQUIRE(cfg.degree >= 1 && cfg.degree <= 3, FEM_ERR_ARG, "operator: degree must be 1, 2 or 3");
   SFEM_REQUIRE(cfg.precision == FEM_FP64 || cfg.precision == FEM_FP32, FEM_ERR_ARG, "operator: bad precision");
   std::unique_ptr<Operator> op;
-  if (cfg.kind == FEM_CG) {
+  if (mesh.curved) {
+    SFEM_REQUIRE(cfg.kind == FEM_CG, FEM_ERR_ARG,
+                 "curved meshes: CG operators only (the DG face terms are affine in this library)");
+    op = make_curved_cg_operator(mesh, cfg);
+  } else if (cfg.kind == FEM_CG) {
     SFEM_REQUIRE(cfg.n_components == 1 || cfg.n_components == 3, FEM_ERR_ARG, "CG: n_components must be 1 or 3");
     if (cfg.n_components == 3) {
       SFEM_REQUIRE(!cfg.weak_bc && (cfg.kernel_variant == 0 || cfg.kernel_variant == 1), FEM_ERR_ARG,

@@ -121,6 +121,8 @@ struct RhsDesc {
 double rhs_value(const RhsDesc& r, const double* x);
 
 std::unique_ptr<Operator> make_operator(const Mesh& mesh, const OpConfig& cfg);
+// CG Laplace on a curved mesh (per-quadrature-point metric, curved.cu)
+std::unique_ptr<Operator> make_curved_cg_operator(const Mesh& mesh, const OpConfig& cfg);
 // Operator on a partition-local mesh it keeps alive: CG takes the given
 // numbering (dofs) and identity rows; DG / Helmholtz read nb == -2 as an
 // interior face whose neighbour is not in the local mesh.

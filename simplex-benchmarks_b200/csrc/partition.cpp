@@ -196,6 +196,7 @@ Partition build_partition(const Mesh& mesh, int degree, int kind, int n_componen
   SFEM_REQUIRE(kind == FEM_CG || kind == FEM_DG || kind == FEM_HELMHOLTZ, FEM_ERR_ARG, "partition: unknown kind");
   SFEM_REQUIRE(n_parts >= 1 && part >= 0 && part < n_parts, FEM_ERR_ARG, "partition: need 0 <= part < n_parts");
   SFEM_REQUIRE(mesh.n_cells >= n_parts, FEM_ERR_ARG, "partition: fewer cells than parts");
+  SFEM_REQUIRE(!mesh.curved, FEM_ERR_ARG, "partition: curved meshes are not partitioned");
   SFEM_REQUIRE(kind == FEM_CG ? n_components == 1 : (n_components == 1 || n_components == 3), FEM_ERR_ARG,
                "partition: n_components must be 1 (CG, DG) or 1 / 3 (Helmholtz)");
   Partition P;

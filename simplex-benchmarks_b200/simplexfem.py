@@ -87,6 +87,8 @@ _PROTOS = [
                                               C.POINTER(C.c_void_p)]),
     ("fem_mesh_read_vtk", C.c_int, [C.c_char_p, C.c_int32, C.POINTER(C.c_void_p)]),
     ("fem_mesh_copy_input_cells", C.c_int, [C.c_void_p, C.c_void_p]),
+    ("fem_mesh_curve", C.c_int, [C.c_void_p, C.c_double]),
+    ("fem_mesh_copy_edge_nodes", C.c_int, [C.c_void_p, C.c_void_p]),
     ("fem_mesh_destroy", C.c_int, [C.c_void_p]),
     ("fem_mesh_sizes", C.c_int, [C.c_void_p] + [C.POINTER(C.c_int64)] * 4),
     ("fem_mesh_copy_vertices", C.c_int, [C.c_void_p, C.c_void_p]),
@@ -251,6 +253,18 @@ class Mesh:
         m._adopt(h)
         m.n = None
         return m
+
+    def curve(self, amplitude):
+        """Curvilinear geometry (fem_mesh_curve): the mesh is moved by a smooth
+        bump that keeps the box boundary and gets quadratic cells."""
+        check(lib().fem_mesh_curve(self.handle, float(amplitude)))
+        return self
+
+    def edge_nodes(self):
+        """Edge geometry nodes of a curved mesh, [n_cells][6][3]."""
+        a = np.empty((self.n_cells, 6, 3), np.float64)
+        check(lib().fem_mesh_copy_edge_nodes(self.handle, a.ctypes.data))
+        return a
 
     def input_cells(self):
         """Input index of every cell (meshes from arrays; identity otherwise)."""
