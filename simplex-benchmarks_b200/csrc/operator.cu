@@ -1041,10 +1041,11 @@ class DGOperator final : public Operator {
   // cells per CTA; 3 warp roles, 32 cells per CTA
   // (measured on B200: scalar P3 runs best register-capped at 64 cells per CTA,
   // the 3-component forms at 128 cells per CTA)
-  // measured on B200 (DG P3 32^3): scalar P3 per cell x64 with 6 CTAs per SM
-  // in FP64 (82.9 us), results in registers with 8 CTAs per SM in FP32 (44.0
-  // against 48.2 us); 128 cells per CTA otherwise
-  static int default_variant(int p, int nc) { return (nc == 1 && p == 3) ? (sizeof(T) == 4 ? 4 : 2) : 1; }
+  // measured on B200 (DG P3 32^3, medians of 25 L2-flushed vmults): FP64
+  // 82.9 us with 128 cells per CTA against 85.0 us with 64; FP32 44.1 us with
+  // the results in registers and 8 CTAs per SM against 52.2 us; 128 cells per
+  // CTA otherwise
+  static int default_variant(int p, int nc) { return (nc == 1 && p == 3 && sizeof(T) == 4) ? 4 : 1; }
 
   static DGBatch<T> make_batch(const DGProblem<T>* probs, int n, int bs, int64_t& n_blocks) {
     DGBatch<T> b;
