@@ -18,7 +18,10 @@ contiguous cell ranges), on the same mesh built by the oracle's own generator
 
 N > 1 (torchrun): every rank runs its own replica of the workload (the
 north-star path is a single-GPU operator; no data-path collective), timing is
-the max over ranks, value is the sum of DoFs over ranks / that time.
+the max over ranks, value is the sum of DoFs over ranks / that time.  With
+--dd the ranks instead share one 32 x 32 x 32N mesh, domain-decomposed, and
+exchange ghost cells over NCCL in every vmult (simplex-benchmarks_b200/
+distributed.py).
 """
 import argparse
 import json
@@ -52,6 +55,9 @@ def parse():
     ap.add_argument("--no-solve", action="store_true", help="skip the multigrid solve measurement")
     ap.add_argument("--no-extra", action="store_true", help="skip the CG (configs 1, 1L) and batch (config 4) lines")
     ap.add_argument("--no-learned", action="store_true", help="skip training and timing the learned smoother")
+    ap.add_argument("--dd", action="store_true",
+                    help="domain decomposition instead of replicas: one 32^3 x 6-tet DG P3 block per rank of a "
+                         "32 x 32 x 32N mesh, halo exchange over NCCL every vmult")
     ap.add_argument("--case", choices=["cg-p2-64", "cg-p1-128", "cg-p2-128", "mlp-64", "dg-p3-32"],
                     help="run one small kernel workload (for profiling) instead of the benchmark")
     ap.add_argument("--variant", type=int, default=0, help="kernel variant of --case dg-p3-32 (0: default)")
@@ -512,6 +518,56 @@ def run_reference(args):
     print(json.dumps(line), flush=True)
 
 
+def run_dd(args):
+    """Weak scaling of the domain-decomposed DG P3 vmult: the mesh is 32 x 32 x
+    32N hexes x 6 tets (jitter 0.1h) split into N contiguous Morton ranges, one
+    per rank; every step is one ghost update (NCCL point-to-point) and one
+    local vmult; time = max over ranks of the device time."""
+    import numpy as np
+    import torch
+    import torch.distributed as dist
+    import simplexfem as sf
+    import distributed as fd
+    rank, world, local = dist_env()
+    torch.cuda.set_device(local)
+    import datetime
+    dist.init_process_group("nccl" if world > 1 else "gloo", timeout=datetime.timedelta(seconds=120),
+                            **({"device_id": torch.device("cuda", local)} if world > 1 else {}))
+    mesh = sf.Mesh((N_HEX, N_HEX, N_HEX * world), jitter=JITTER, seed=0)
+    dop = fd.DistributedOperator(mesh, DEGREE, "dg", "fp64")
+    xg = torch.tensor(np.random.default_rng(1).uniform(-1.0, 1.0, dop.partition.n_global), device="cuda")
+    x = dop.scatter(xg)
+    y = dop.initialize_dof_vector()
+    flush_buf = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")
+    for _ in range(args.warmup):
+        dop.vmult(y, x)
+    dist.barrier()
+    torch.cuda.synchronize()
+    total = 0.0
+    for _ in range(args.steps):
+        flush_buf.fill_(1.0)
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record()
+        dop.vmult(y, x)
+        b.record()
+        torch.cuda.synchronize()
+        total += a.elapsed_time(b)
+    dist.barrier()
+    total_ms = max_over_ranks(total, "cuda")
+    value = dop.partition.n_global * args.steps / (total_ms / 1e3)
+    if rank == 0:
+        line = {"metric": METRIC, "value": value, "unit": "DoF/s", "n_gpus": world, "steps": args.steps,
+                "warmup": args.warmup, "ms_per_step": total_ms / args.steps, "higher_is_better": True,
+                "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+                "config": {"workload": f"DG SIPG Poisson vmult, P3 on 32 x 32 x {32 * world} x 6 Kuhn tets, "
+                                       f"domain-decomposed over {world} ranks", "parallelism": f"dd{world}",
+                           "l2": "flushed (256 MB write) before every timed vmult"},
+                "gpu_launches": 2 * args.steps}
+        print(json.dumps(line), flush=True)
+    dist.barrier()
+    dist.destroy_process_group()
+
+
 def run_ours(args):
     import numpy as np
     import torch
@@ -701,6 +757,8 @@ def main():
         return
     if args.impl == "reference":
         run_reference(args)
+    elif args.dd:
+        run_dd(args)
     else:
         run_ours(args)
 
