@@ -51,7 +51,7 @@ struct DGProblem {
   const int8_t* nbf;  // [4][n_cells]
   const T* src;       // [n_cells][NC][K]
   T* dst;
-  T* Q;               // [n_cells][4][NC][NFQ]
+  T* Q;               // [n_cells][4][NC][NFQ], or block-major (see dg_trace_blk_kernel)
   int64_t n_cells;
 };
 
@@ -167,6 +167,94 @@ __device__ __forceinline__ void stage_out(T* __restrict__ g, const T* __restrict
   for (int e = threadIdx.x; e < total; e += BS) g[e] = sm[(e / N) * S + (e % N)];
 }
 
+// ---- block-major traces (scalar problems) ------------------------------------------------------
+// The staged forms below publish traces as rows [cell][4][NC][NFQ].  For
+// scalar problems the one-thread-per-cell forms store them block-major,
+//   Q[b][k][l]: block b of kQB = 128 cells, trace k = f * NFQ + m, local cell l,
+// so that the trace pass needs no shared memory (each thread reads its own
+// row with 16-byte loads and every trace k is one coalesced store across the
+// block), the apply pass copies its CTA's traces as QN contiguous runs, and a
+// thread's own traces sit at stride BS in shared memory (bank-conflict free).
+// A neighbour in another block is read at Q[nb / 128][k][nb % 128].
+constexpr int kQB = 128;
+
+// N values from p into v: 16-byte loads when p and the row allow it
+template <int N, typename T>
+__device__ __forceinline__ void load_row(const T* __restrict__ p, T (&v)[N]) {
+  constexpr int V = 16 / int(sizeof(T));
+  if constexpr (N % V == 0) {
+    if ((reinterpret_cast<uintptr_t>(p) & 15u) == 0) {
+#pragma unroll
+      for (int k = 0; k < N / V; ++k) {
+        const uint4 w = __ldg(reinterpret_cast<const uint4*>(p) + k);
+        const T* e = reinterpret_cast<const T*>(&w);
+#pragma unroll
+        for (int q = 0; q < V; ++q) v[k * V + q] = e[q];
+      }
+      return;
+    }
+  }
+#pragma unroll
+  for (int i = 0; i < N; ++i) v[i] = __ldg(p + i);
+}
+
+// Traces of the CTA's cells c0 .. c0 + nloc - 1 (BS cells inside one block of
+// kQB, c0 a multiple of BS) into shared memory [QN][BS]; all loads in flight
+// before the first store.
+template <int QN, int BS, typename T>
+__device__ __forceinline__ void stage_q_blk(T* __restrict__ sq, const T* __restrict__ Q, int64_t c0, int nloc) {
+  static_assert(kQB % BS == 0, "a CTA's cells lie in one trace block");
+  const T* base = Q + (c0 / kQB) * (QN * kQB) + (c0 % kQB);
+  const int l = threadIdx.x;
+  if (l < nloc) {
+    T v[QN];
+#pragma unroll
+    for (int k = 0; k < QN; ++k) v[k] = __ldg(base + k * kQB + l);
+#pragma unroll
+    for (int k = 0; k < QN; ++k) sq[k * BS + l] = v[k];
+  }
+}
+
+// trace k of `cell` in the block-major layout
+template <int QN, typename T>
+__device__ __forceinline__ const T* q_blk_ptr(const T* Q, int64_t cell, int k) {
+  return Q + (cell / kQB) * (QN * kQB) + int64_t(k) * kQB + cell % kQB;
+}
+
+// Pass 1 for scalar problems, block-major: one thread per cell, no shared memory.
+template <int P, typename T>
+__global__ void __launch_bounds__(kQB) dg_trace_blk_kernel(const __grid_constant__ DGBatch<T> batch,
+                                                           int64_t n_blocks) {
+  using O = gen::Ops<P>;
+  constexpr int K = O::K, KQ = O::KQ, NFQ = O::NFQ, QN = 4 * NFQ;
+  for (int64_t blk = blockIdx.x; blk < n_blocks; blk += gridDim.x) {
+    const int pi = find_problem(batch, blk);
+    const DGProblem<T>& pr = batch.p[pi];
+    const int64_t lb = blk - batch.block_begin[pi];
+    const int64_t c = lb * kQB + threadIdx.x;
+    if (c >= pr.n_cells) continue;
+    const int64_t n = pr.n_cells;
+    T G[6];
+#pragma unroll
+    for (int k = 0; k < 6; ++k) G[k] = __ldg(pr.geo + k * n + c);
+    T u[K];
+    load_row<K>(pr.src + c * K, u);
+    T g[3 * KQ];
+    O::grad(u, g);
+    T* q = pr.Q + lb * (QN * kQB) + threadIdx.x;
+#pragma unroll
+    for (int f = 0; f < 4; ++f) {
+      T cf[3];
+      face_cf(G, f, cf);
+#pragma unroll
+      for (int m = 0; m < NFQ; ++m) {
+        const int nq = O::fnq(f, m);
+        q[(f * NFQ + m) * kQB] = cf[0] * g[nq] + cf[1] * g[KQ + nq] + cf[2] * g[2 * KQ + nq];
+      }
+    }
+  }
+}
+
 // Publish q_f = 2|F_f| d_n u (own outward normal) at the P_{p-1} nodes of every face.
 template <int P, int NC, int BS, typename T>
 __global__ void __launch_bounds__(BS) dg_trace_kernel(const __grid_constant__ DGBatch<T> batch, int64_t n_blocks) {
@@ -222,7 +310,10 @@ __global__ void __launch_bounds__(BS) dg_trace_kernel(const __grid_constant__ DG
 // XS: `xs` points at this cell's staged cross-block neighbour data, one row
 // of XROW values per face slot (slot[f] < 0: not staged): the neighbour's
 // face values already in this cell's face-node order, then its traces.
-template <int P, int NC, bool MASS, bool HAVE_NB, typename T, bool XS = false>
+// BQ (scalar): the traces are block-major, staged as [QN][BSQ] (qs = sq + this
+// cell's local index), and a neighbour in another block is read from pr.Q in
+// the block-major layout.
+template <int P, int NC, bool MASS, bool HAVE_NB, typename T, bool XS = false, bool BQ = false, int BSQ = 1>
 __device__ __forceinline__ void dg_cell_component(const DGProblem<T>& pr, int64_t c0, int comp,
                                                   const T* us, const T* qs, const T* su, const T* sq, int nloc,
                                                   const T (&G)[6], const T (&sf)[4], T md,
@@ -232,6 +323,8 @@ __device__ __forceinline__ void dg_cell_component(const DGProblem<T>& pr, int64_
   using O = gen::Ops<P>;
   using S = DGShape<P, NC>;
   constexpr int K = O::K, KQ = O::KQ, NF = O::NF, NFQ = O::NFQ;
+  static_assert(!BQ || NC == 1, "block-major traces are for scalar problems");
+  constexpr int QST = BQ ? BSQ : 1;  // stride of a cell's consecutive traces in shared memory
   const T* u = us + comp * K;
   T h[3 * KQ];
   {
@@ -252,7 +345,7 @@ __device__ __forceinline__ void dg_cell_component(const DGProblem<T>& pr, int64_
   for (int f = 0; f < 4; ++f) {
     T cf[3];
     face_cf(G, f, cf);
-    const T* qm = qs + (f * NC + comp) * NFQ;
+    const T* qm = qs + (BQ ? f * NFQ * BSQ : (f * NC + comp) * NFQ);
     T j[NF], avg[NFQ];
     if (nb[f] >= 0) {
       if (XS && (*slot)[f] >= 0) {
@@ -260,34 +353,38 @@ __device__ __forceinline__ void dg_cell_component(const DGProblem<T>& pr, int64_
 #pragma unroll
         for (int i = 0; i < NF; ++i) j[i] = u[O::fn(f, i)] - xn[i];
 #pragma unroll
-        for (int m = 0; m < NFQ; ++m) avg[m] = T(0.25) * (qm[m] - xn[NF + m]);
+        for (int m = 0; m < NFQ; ++m) avg[m] = T(0.25) * (qm[m * QST] - xn[NF + m]);
       } else if (HAVE_NB) {
         const int64_t lc = int64_t(nb[f]) - c0;
         const T* un;
         const T* qn;
+        int qns;  // stride of the neighbour's consecutive traces
         if (lc >= 0 && lc < nloc) {
           un = su + lc * S::US + comp * K;
-          qn = sq + lc * S::QS + (nbf[f] * NC + comp) * NFQ;
+          qn = BQ ? sq + nbf[f] * NFQ * BSQ + lc : sq + lc * S::QS + (nbf[f] * NC + comp) * NFQ;
+          qns = QST;
         } else {
           un = pr.src + (int64_t(nb[f]) * NC + comp) * K;
-          qn = pr.Q + ((int64_t(nb[f]) * 4 + nbf[f]) * NC + comp) * NFQ;
+          qn = BQ ? q_blk_ptr<4 * NFQ>(pr.Q, nb[f], nbf[f] * NFQ)
+                  : pr.Q + ((int64_t(nb[f]) * 4 + nbf[f]) * NC + comp) * NFQ;
+          qns = BQ ? kQB : 1;
         }
 #pragma unroll
         for (int i = 0; i < NF; ++i) j[i] = u[O::fn(f, i)] - un[O::fn_runtime(nbf[f], i)];
 #pragma unroll
-        for (int m = 0; m < NFQ; ++m) avg[m] = T(0.25) * (qm[m] - qn[m]);
+        for (int m = 0; m < NFQ; ++m) avg[m] = T(0.25) * (qm[m * QST] - qn[m * qns]);
       } else {
 #pragma unroll
         for (int i = 0; i < NF; ++i) j[i] = u[O::fn(f, i)];
 #pragma unroll
-        for (int m = 0; m < NFQ; ++m) avg[m] = T(0.25) * qm[m];
+        for (int m = 0; m < NFQ; ++m) avg[m] = T(0.25) * qm[m * QST];
       }
     } else {
       // boundary face: u+ = -u-, d_n u+ = d_n u-
 #pragma unroll
       for (int i = 0; i < NF; ++i) j[i] = T(2) * u[O::fn(f, i)];
 #pragma unroll
-      for (int m = 0; m < NFQ; ++m) avg[m] = T(0.5) * qm[m];
+      for (int m = 0; m < NFQ; ++m) avg[m] = T(0.5) * qm[m * QST];
     }
     // value test: sigma|F| MFPP j - MFPQ avg
     T t[NF];
@@ -340,7 +437,9 @@ __device__ __forceinline__ void load_cell(const DGProblem<T>& pr, int64_t c, Cel
 // results stay in registers until every thread of the CTA is done reading the
 // staged src rows, then reuse those rows for the coalesced write-out, so the
 // CTA needs no separate result rows (less shared memory, more CTAs per SM).
-template <int P, int NC, bool MASS, int BS, typename T, int MINB = (BS == 64 ? 6 : 1), bool ALIAS = false>
+// BQ (NC == 1): block-major traces (dg_trace_blk_kernel), staged as [QN][BS].
+template <int P, int NC, bool MASS, int BS, typename T, int MINB = (BS == 64 ? 6 : 1), bool ALIAS = false,
+          bool BQ = false>
 __global__ void __launch_bounds__(BS, MINB) dg_apply_kernel(const __grid_constant__ DGBatch<T> batch,
                                                             int64_t n_blocks) {
   using O = gen::Ops<P>;
@@ -357,16 +456,18 @@ __global__ void __launch_bounds__(BS, MINB) dg_apply_kernel(const __grid_constan
     const int nloc = int(pr.n_cells - c0 < BS ? pr.n_cells - c0 : int64_t(BS));
     __syncthreads();
     stage_in<S::U, S::US, BS>(su, pr.src + c0 * S::U, nloc);
-    stage_in<S::QN, S::QS, BS>(sq, pr.Q + c0 * S::QN, nloc);
+    if constexpr (BQ) stage_q_blk<S::QN, BS>(sq, pr.Q, c0, nloc);
+    else stage_in<S::QN, S::QS, BS>(sq, pr.Q + c0 * S::QN, nloc);
     __syncthreads();
     const int t = threadIdx.x;
+    const T* qs = BQ ? sq + t : sq + t * S::QS;  // this cell's traces
     if (ALIAS) {
       T y[O::K];
       if (t < nloc) {
         CellData<T> d;
         load_cell<MASS>(pr, c0 + t, d);
-        dg_cell_component<P, NC, MASS, true>(pr, c0, 0, su + t * S::US, sq + t * S::QS, su, sq, nloc, d.G, d.sf,
-                                             d.md, d.nb, d.nbf, y);
+        dg_cell_component<P, NC, MASS, true, T, false, BQ, BS>(pr, c0, 0, su + t * S::US, qs, su, sq, nloc, d.G,
+                                                                d.sf, d.md, d.nb, d.nbf, y);
       }
       __syncthreads();  // every thread is done with the staged src rows
       if (t < nloc) {
@@ -379,8 +480,8 @@ __global__ void __launch_bounds__(BS, MINB) dg_apply_kernel(const __grid_constan
 #pragma unroll 1
       for (int comp = 0; comp < NC; ++comp) {
         T y[O::K];
-        dg_cell_component<P, NC, MASS, true>(pr, c0, comp, su + t * S::US, sq + t * S::QS, su, sq, nloc, d.G,
-                                             d.sf, d.md, d.nb, d.nbf, y);
+        dg_cell_component<P, NC, MASS, true, T, false, BQ, BS>(pr, c0, comp, su + t * S::US, qs, su, sq, nloc, d.G,
+                                                                d.sf, d.md, d.nb, d.nbf, y);
 #pragma unroll
         for (int i = 0; i < O::K; ++i) sy[t * S::US + comp * O::K + i] = y[i];
       }

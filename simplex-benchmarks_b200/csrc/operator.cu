@@ -890,7 +890,8 @@ class DGOperator final : public Operator {
   DevBuf<T> d_geo;      // [6 + 4 + (mass?1:0)][n_cells]
   DevBuf<int32_t> d_nb; // [4][n_cells]
   DevBuf<int8_t> d_nbf; // [4][n_cells]
-  DevBuf<T> d_Q;        // [n_cells][4][NC][NFQ] published face normal derivatives
+  DevBuf<T> d_Q;        // published face normal derivatives: [n_cells][4][NC][NFQ], or block-major
+                        // (scalar problems, 1-thread-per-cell forms), for whole 128-cell blocks
   bool has_mass = false;
 
   DGOperator(const Mesh& mesh, const OpConfig& c) {
@@ -966,7 +967,7 @@ class DGOperator final : public Operator {
       }
     d_nb.upload(nb);
     d_nbf.upload(nbf);
-    d_Q.alloc(size_t(n_cells) * 4 * cfg.n_components * nfq_of(p));
+    d_Q.alloc(size_t((n_cells + kQB - 1) / kQB * kQB) * 4 * cfg.n_components * nfq_of(p));
   }
 
   DGProblem<T> problem(const void* src, void* dst) const {
@@ -1075,10 +1076,20 @@ class DGOperator final : public Operator {
     const size_t sm_trace = size_t(BS) * (S::US + S::QS) * sizeof(T);
     const size_t sm_apply = size_t(BS) * ((ALIAS ? 1 : 2) * S::US + S::QS) * sizeof(T);
     static std::atomic<uint64_t> conf_t{0}, conf_a{0};
-    auto apply = dg_apply_kernel<P, NC, MASS, BS, T, MINB, ALIAS>;
-    opt_in_smem(dg_trace_kernel<P, NC, BS, T>, sm_trace, conf_t);
+    // scalar problems: block-major traces (no shared memory in the trace pass)
+    constexpr bool BQ = NC == 1;
+    auto apply = dg_apply_kernel<P, NC, MASS, BS, T, MINB, ALIAS, BQ>;
     opt_in_smem(apply, sm_apply, conf_a);
-    if (what != 2) dg_trace_kernel<P, NC, BS, T><<<unsigned(n_blocks), BS, sm_trace, s>>>(b, n_blocks);
+    if (what != 2) {
+      if constexpr (BQ) {
+        int64_t nbt = 0;
+        const DGBatch<T> bt = make_batch(probs, n, kQB, nbt);
+        dg_trace_blk_kernel<P, T><<<unsigned(nbt), kQB, 0, s>>>(bt, nbt);
+      } else {
+        opt_in_smem(dg_trace_kernel<P, NC, BS, T>, sm_trace, conf_t);
+        dg_trace_kernel<P, NC, BS, T><<<unsigned(n_blocks), BS, sm_trace, s>>>(b, n_blocks);
+      }
+    }
     if (what != 1) apply<<<unsigned(n_blocks), BS, sm_apply, s>>>(b, n_blocks);
   }
 
