@@ -39,6 +39,7 @@
 
 #include "kernels_cg.cuh"
 #include "ref_kernels.cuh"
+#include "tcgen05.cuh"
 
 namespace sfem {
 
@@ -252,6 +253,133 @@ __global__ void __launch_bounds__(kQB) dg_trace_blk_kernel(const __grid_constant
         q[(f * NFQ + m) * kQB] = cf[0] * g[nq] + cf[1] * g[KQ + nq] + cf[2] * g[2 * KQ + nq];
       }
     }
+  }
+}
+
+// ---- the same pass fed by bulk copies ----------------------------------------------------------
+// Persistent CTAs of kQB threads; a ring of NS stages, each holding one
+// block's src rows ([kQB][K], dense) and its metric ([6][kQB]).  Thread 0
+// issues cp.async.bulk copies (global -> shared, no multicast, completion on
+// the stage's mbarrier) for block k + NS as soon as every thread is done with
+// block k, so NS blocks are always in flight while one computes.  The host
+// uses it when every copy starts 16-byte aligned and moves whole 16-byte units
+// (src rows of the last block included; the metric copies are whole blocks,
+// which the geometry's rows past the metric keep inside the allocation).
+// Every mbarrier wait is bounded: on a timeout the CTA stops, waits (bounded)
+// for the copies it issued and sets *status.
+template <typename T, int K, int NS>
+struct TraceTmaShape {
+  static constexpr int U_BYTES = kQB * K * int(sizeof(T));
+  static constexpr int G_BYTES = 6 * kQB * int(sizeof(T));
+  static constexpr int STAGE = U_BYTES + G_BYTES;
+  static constexpr int OFF_BAR = NS * STAGE;
+  static constexpr int SMEM = OFF_BAR + 8 * NS;
+  static_assert(U_BYTES % 16 == 0 && G_BYTES % 16 == 0, "bulk copies move 16-byte units");
+};
+
+__device__ __forceinline__ void mbar_init(uint32_t bar, uint32_t count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(bar), "r"(count) : "memory");
+}
+__device__ __forceinline__ void mbar_expect_tx(uint32_t bar, uint32_t bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar), "r"(bytes) : "memory");
+}
+// global -> shared bulk copy without multicast, completion counted on `bar`
+__device__ __forceinline__ void bulk_g2s(uint32_t dst, const void* src, uint32_t bytes, uint32_t bar) {
+  asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(dst),
+               "l"(src), "r"(bytes), "r"(bar)
+               : "memory");
+}
+
+template <int P, typename T, int NS>
+__global__ void __launch_bounds__(kQB) dg_trace_tma_kernel(const __grid_constant__ DGBatch<T> batch, int64_t n_blocks,
+                                                           int* __restrict__ status) {
+  using O = gen::Ops<P>;
+  constexpr int K = O::K, KQ = O::KQ, NFQ = O::NFQ, QN = 4 * NFQ;
+  using S = TraceTmaShape<T, K, NS>;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  const int t = threadIdx.x;
+  const uint32_t bar0 = tc::smem_u32(smem_raw + S::OFF_BAR);
+  const int64_t first = blockIdx.x, stride = gridDim.x;
+  const int64_t mine = first < n_blocks ? (n_blocks - 1 - first) / stride + 1 : 0;
+  // thread 0: copies of this CTA's k-th block into stage k % NS
+  auto issue = [&](int64_t k) {
+    const int64_t blk = first + k * stride;
+    const int pi = find_problem(batch, blk);
+    const DGProblem<T>& pr = batch.p[pi];
+    const int64_t c0 = (blk - batch.block_begin[pi]) * kQB;
+    const int64_t rest = pr.n_cells - c0;
+    const uint32_t ub = uint32_t(rest < kQB ? rest : int64_t(kQB)) * K * sizeof(T);
+    const int s = int(k % NS);
+    unsigned char* st = smem_raw + s * S::STAGE;
+    const uint32_t bar = bar0 + 8 * s;
+    mbar_expect_tx(bar, ub + S::G_BYTES);
+    bulk_g2s(tc::smem_u32(st), pr.src + c0 * K, ub, bar);
+#pragma unroll
+    for (int i = 0; i < 6; ++i)
+      bulk_g2s(tc::smem_u32(st + S::U_BYTES + i * kQB * sizeof(T)), pr.geo + i * pr.n_cells + c0,
+               kQB * sizeof(T), bar);
+  };
+  if (t == 0) {
+    for (int s = 0; s < NS; ++s) mbar_init(bar0 + 8 * s, 1);
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    for (int64_t k = 0; k < NS && k < mine; ++k) issue(k);
+  }
+  __syncthreads();
+  int64_t done = 0;  // blocks whose stage wait completed
+  bool ok = true;
+  for (int64_t k = 0; k < mine; ++k) {
+    const int s = int(k % NS);
+    if (!tc::bar_wait(bar0 + 8 * s, uint32_t((k / NS) & 1))) ok = false;
+    if (!__syncthreads_and(ok)) {
+      ok = false;
+      break;
+    }
+    done = k + 1;
+    const int64_t blk = first + k * stride;
+    const int pi = find_problem(batch, blk);
+    const DGProblem<T>& pr = batch.p[pi];
+    const int64_t lb = blk - batch.block_begin[pi];
+    if (lb * kQB + t < pr.n_cells) {
+      const T* su = reinterpret_cast<const T*>(smem_raw + s * S::STAGE);
+      const T* sg = reinterpret_cast<const T*>(smem_raw + s * S::STAGE + S::U_BYTES);
+      T G[6];
+#pragma unroll
+      for (int i = 0; i < 6; ++i) G[i] = sg[i * kQB + t];
+      T u[K];
+      constexpr int V = 16 / int(sizeof(T));
+      if constexpr ((K * sizeof(T)) % 16 == 0) {
+#pragma unroll
+        for (int q = 0; q < K / V; ++q) {
+          const uint4 w = reinterpret_cast<const uint4*>(su + t * K)[q];
+          const T* e = reinterpret_cast<const T*>(&w);
+#pragma unroll
+          for (int r = 0; r < V; ++r) u[q * V + r] = e[r];
+        }
+      } else {
+#pragma unroll
+        for (int i = 0; i < K; ++i) u[i] = su[t * K + i];
+      }
+      T g[3 * KQ];
+      O::grad(u, g);
+      T* q = pr.Q + lb * (QN * kQB) + t;
+#pragma unroll
+      for (int f = 0; f < 4; ++f) {
+        T cf[3];
+        face_cf(G, f, cf);
+#pragma unroll
+        for (int m = 0; m < NFQ; ++m) {
+          const int nq = O::fnq(f, m);
+          q[(f * NFQ + m) * kQB] = cf[0] * g[nq] + cf[1] * g[KQ + nq] + cf[2] * g[2 * KQ + nq];
+        }
+      }
+    }
+    __syncthreads();  // stage s is free
+    if (t == 0 && k + NS < mine) issue(k + NS);
+  }
+  if (!ok && t == 0) {
+    // wait (bounded) for the copies still in flight, then report
+    for (int64_t k = done; k < mine && k < done + NS; ++k) tc::bar_wait(bar0 + 8 * int(k % NS), uint32_t((k / NS) & 1));
+    atomicExch(status, 1);
   }
 }
 

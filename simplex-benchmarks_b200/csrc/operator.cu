@@ -892,6 +892,7 @@ class DGOperator final : public Operator {
   DevBuf<int8_t> d_nbf; // [4][n_cells]
   DevBuf<T> d_Q;        // published face normal derivatives: [n_cells][4][NC][NFQ], or block-major
                         // (scalar problems, 1-thread-per-cell forms), for whole 128-cell blocks
+  DevBuf<int> d_status; // timeouts of the bounded waits in the bulk-copy trace pass
   bool has_mass = false;
 
   DGOperator(const Mesh& mesh, const OpConfig& c) {
@@ -968,6 +969,15 @@ class DGOperator final : public Operator {
     d_nb.upload(nb);
     d_nbf.upload(nbf);
     d_Q.alloc(size_t((n_cells + kQB - 1) / kQB * kQB) * 4 * cfg.n_components * nfq_of(p));
+    d_status.alloc(1);
+    SFEM_CUDA(cudaMemset(d_status.p, 0, sizeof(int)));
+  }
+
+  int status(bool clear) override {
+    int v = 0;
+    SFEM_CUDA(cudaMemcpy(&v, d_status.p, sizeof(int), cudaMemcpyDeviceToHost));
+    if (clear && v) SFEM_CUDA(cudaMemset(d_status.p, 0, sizeof(int)));
+    return v;
   }
 
   DGProblem<T> problem(const void* src, void* dst) const {
@@ -984,12 +994,12 @@ class DGOperator final : public Operator {
 
   void vmult(void* dst, const void* src, cudaStream_t s) override {
     const DGProblem<T> pr = problem(src, dst);
-    launch_dg(cfg, &pr, 1, s, 0);
+    launch_dg(cfg, &pr, 1, s, 0, d_status.p);
   }
 
   void vmult_phase(void* dst, const void* src, int phase, cudaStream_t s) override {
     const DGProblem<T> pr = problem(src, dst);
-    launch_dg(cfg, &pr, 1, s, phase);
+    launch_dg(cfg, &pr, 1, s, phase, d_status.p);
   }
 
   size_t scratch_bytes() const override { return d_Q.n * sizeof(T); }
@@ -998,12 +1008,12 @@ class DGOperator final : public Operator {
     SFEM_REQUIRE(bytes >= scratch_bytes(), FEM_ERR_ARG, "vmult: scratch too small");
     DGProblem<T> pr = problem(src, dst);
     pr.Q = static_cast<T*>(scratch);
-    launch_dg(cfg, &pr, 1, s, 0);
+    launch_dg(cfg, &pr, 1, s, 0, d_status.p);
   }
 
   void diagonal(void* diag, cudaStream_t s) override {
     const DGProblem<T> pr = problem(nullptr, diag);
-    launch_dg(cfg, &pr, 1, s, 3);
+    launch_dg(cfg, &pr, 1, s, 3, d_status.p);
   }
 
   void work(double& flops, double& bytes) const override {
@@ -1019,7 +1029,9 @@ class DGOperator final : public Operator {
   }
 
   // Dispatch over n problems.  what: 0 trace+apply, 1 trace, 2 apply, 3 diagonal.
-  static void launch_dg(const OpConfig& cfg, const DGProblem<T>* probs, int n, cudaStream_t s, int what) {
+  // status: device word set by the bounded waits of the bulk-copy trace pass.
+  static void launch_dg(const OpConfig& cfg, const DGProblem<T>* probs, int n, cudaStream_t s, int what,
+                        int* status) {
     const bool mass = cfg.kind == FEM_HELMHOLTZ;
     const int nc = cfg.n_components;
     SFEM_REQUIRE(nc == 1 || nc == 3, FEM_ERR_ARG, "DG: n_components must be 1 or 3");
@@ -1027,7 +1039,7 @@ class DGOperator final : public Operator {
     const int variant = cfg.kernel_variant > 0 ? cfg.kernel_variant : default_variant(cfg.degree, nc);
 #define SFEM_DG_CASE(P, NC, MASS)                                                       \
   if (cfg.degree == P && nc == NC && mass == MASS) {                                    \
-    run<P, NC, MASS>(probs, n, s, what, variant);                                       \
+    run<P, NC, MASS>(probs, n, s, what, variant, status);                               \
     return;                                                                             \
   }
     SFEM_DG_CASE(1, 1, false) SFEM_DG_CASE(2, 1, false) SFEM_DG_CASE(3, 1, false)
@@ -1068,8 +1080,42 @@ class DGOperator final : public Operator {
       SFEM_CUDA(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, int(bytes)));
   }
 
+  // The bulk-copy trace pass needs every copy 16-byte aligned and a whole
+  // number of 16-byte units: src rows (the last block's included) and the
+  // metric rows of the geometry.
+  template <int P>
+  static bool trace_tma_ok(const DGProblem<T>* probs, int n) {
+    for (int i = 0; i < n; ++i) {
+      const DGProblem<T>& pr = probs[i];
+      if ((reinterpret_cast<uintptr_t>(pr.src) | reinterpret_cast<uintptr_t>(pr.geo)) & 15u) return false;
+      if ((size_t(pr.n_cells) * sizeof(T)) % 16 != 0) return false;  // metric row starts
+      if ((size_t(pr.n_cells % kQB) * k_of(P) * sizeof(T)) % 16 != 0) return false;
+    }
+    return true;
+  }
+  template <int P>
+  static void run_trace_tma(const DGBatch<T>& b, int64_t n_blocks, cudaStream_t s, int* status) {
+    constexpr int NS = 3;
+    using S = TraceTmaShape<T, gen::Ops<P>::K, NS>;
+    auto kern = dg_trace_tma_kernel<P, T, NS>;
+    static std::atomic<uint64_t> conf{0};
+    static int grid_per_dev[64] = {};
+    int dev = 0;
+    SFEM_CUDA(cudaGetDevice(&dev));
+    if (first_use_on_device(conf, dev)) {
+      SFEM_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, S::SMEM));
+      int sms = 0, occ = 0;
+      SFEM_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+      SFEM_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, kern, kQB, S::SMEM));
+      SFEM_REQUIRE(occ > 0, FEM_ERR_CUDA, "DG trace pass does not fit on an SM");
+      grid_per_dev[dev] = sms * occ;
+    }
+    const int64_t grid = std::max<int64_t>(1, std::min<int64_t>(n_blocks, grid_per_dev[dev]));
+    kern<<<unsigned(grid), kQB, S::SMEM, s>>>(b, n_blocks, status);
+  }
+
   template <int P, int NC, bool MASS, int BS, int MINB = (BS == 64 ? 6 : 1), bool ALIAS = false>
-  static void run_cell(const DGProblem<T>* probs, int n, cudaStream_t s, int what) {
+  static void run_cell(const DGProblem<T>* probs, int n, cudaStream_t s, int what, int* status) {
     using S = DGShape<P, NC>;
     int64_t n_blocks = 0;
     const DGBatch<T> b = make_batch(probs, n, BS, n_blocks);
@@ -1084,7 +1130,8 @@ class DGOperator final : public Operator {
       if constexpr (BQ) {
         int64_t nbt = 0;
         const DGBatch<T> bt = make_batch(probs, n, kQB, nbt);
-        dg_trace_blk_kernel<P, T><<<unsigned(nbt), kQB, 0, s>>>(bt, nbt);
+        if (trace_tma_ok<P>(probs, n)) run_trace_tma<P>(bt, nbt, s, status);
+        else dg_trace_blk_kernel<P, T><<<unsigned(nbt), kQB, 0, s>>>(bt, nbt);
       } else {
         opt_in_smem(dg_trace_kernel<P, NC, BS, T>, sm_trace, conf_t);
         dg_trace_kernel<P, NC, BS, T><<<unsigned(n_blocks), BS, sm_trace, s>>>(b, n_blocks);
@@ -1143,25 +1190,25 @@ class DGOperator final : public Operator {
   }
 
   template <int P, int NC, bool MASS>
-  static void run(const DGProblem<T>* probs, int n, cudaStream_t s, int what, int variant) {
+  static void run(const DGProblem<T>* probs, int n, cudaStream_t s, int what, int variant, int* status) {
     if (what == 3) {
       int64_t n_blocks = 0;
       const DGBatch<T> b = make_batch(probs, n, 128, n_blocks);
       dg_diagonal_kernel<P, NC, MASS, T><<<unsigned(n_blocks), 128, 0, s>>>(b, n_blocks);
     } else if (variant == 1) {
-      run_cell<P, NC, MASS, 128>(probs, n, s, what);
+      run_cell<P, NC, MASS, 128>(probs, n, s, what, status);
     } else if (variant == 2) {
-      run_cell<P, NC, MASS, 64>(probs, n, s, what);
+      run_cell<P, NC, MASS, 64>(probs, n, s, what, status);
     } else if (variant == 3) {
       run_warp<P, NC, MASS>(probs, n, s, what);
     } else if (variant == 5) {
       // 64 cells per CTA, 5 CTAs per SM (up to 204 registers: no spills for P3)
-      run_cell<P, NC, MASS, 64, 5, false>(probs, n, s, what);
+      run_cell<P, NC, MASS, 64, 5, false>(probs, n, s, what, status);
     } else if (variant == 4) {
       // 64 cells per CTA, results aliased onto the staged src rows (scalar
       // problems), registers capped for 8 CTAs per SM
-      if (NC == 1) run_cell<P, NC, MASS, 64, 8, (NC == 1)>(probs, n, s, what);
-      else run_cell<P, NC, MASS, 64, 8, false>(probs, n, s, what);
+      if (NC == 1) run_cell<P, NC, MASS, 64, 8, (NC == 1)>(probs, n, s, what, status);
+      else run_cell<P, NC, MASS, 64, 8, false>(probs, n, s, what, status);
     } else if (variant == 7 || variant == 9) {
       // phase-split scalar kernels (kernels_dg2.cuh): 7 results in registers,
       // 64 cells x 5 CTAs per SM; 9 results in shared memory, 64 cells x 4
@@ -1170,13 +1217,13 @@ class DGOperator final : public Operator {
         if (variant == 7) run_split<P, MASS, 64, 5>(probs, n, s, what);
         else run_split<P, MASS, 64, 4, true>(probs, n, s, what);
       } else {
-        run_cell<P, NC, MASS, 128>(probs, n, s, what);
+        run_cell<P, NC, MASS, 128>(probs, n, s, what, status);
       }
     } else if (variant == 11) {
       // 128 cells per CTA with the cross-block neighbour data prefetched into
       // shared memory; multi-component and mass problems take the 128-cell form
       if constexpr (NC == 1 && !MASS) run_xp<P, 128, 192>(probs, n, s, what);
-      else run_cell<P, NC, MASS, 128>(probs, n, s, what);
+      else run_cell<P, NC, MASS, 128>(probs, n, s, what, status);
     } else {
       throw Error(FEM_ERR_ARG, "DG: kernel variant must be 0..5, 7, 9 or 11");
     }
@@ -1220,7 +1267,7 @@ class DGBatchImpl final : public Batch {
       probs[i] = ops[i]->problem(src[i], dst[i]);
       if (q_of[i] >= 0) probs[i].Q = extra_q[q_of[i]].p;
     }
-    DGOperator<T>::launch_dg(cfg, probs, int(ops.size()), s, 0);
+    DGOperator<T>::launch_dg(cfg, probs, int(ops.size()), s, 0, ops[0]->d_status.p);
   }
   int variant() const override { return cfg.kernel_variant; }
   void set_variant(int v) override {
