@@ -60,9 +60,10 @@ def parse():
     ap.add_argument("--dd", action="store_true",
                     help="domain decomposition instead of replicas: one 32^3 x 6-tet DG P3 block per rank of a "
                          "32 x 32 x 32N mesh, halo exchange over NCCL every vmult")
-    ap.add_argument("--case", choices=["cg-p2-64", "cg-p1-128", "cg-p2-128", "mlp-64", "dg-p3-32"],
+    ap.add_argument("--case", choices=["cg-p2-64", "cg-p3-64", "cg-p1-128", "cg-p2-128", "mlp-64", "dg-p3-32"],
                     help="run one small kernel workload (for profiling) instead of the benchmark")
-    ap.add_argument("--variant", type=int, default=0, help="kernel variant of --case dg-p3-32 (0: default)")
+    ap.add_argument("--variant", type=int, default=0,
+                    help="kernel variant of --case dg-p3-32, or of the FP32 operator of a cg-* case (0: default)")
     return ap.parse_args()
 
 
@@ -720,11 +721,13 @@ def run_ours(args):
 
 def run_case(name, reps=3, variant=0):
     """One small workload of a single kernel family, for profiling (ncu -k ...):
-    cg-p2-64 / cg-p1-128 / cg-p2-128: CG vmults (default kernel variant, FP64 and
+    cg-p2-64 / cg-p3-64 / cg-p1-128 / cg-p2-128: CG vmults (default kernel variant, FP64 and
     FP32) on 64^3 or 128^3 x 6 tets, jitter 0.1h; mlp-64: eager V-cycles of the
     mixed multigrid with the learned finest-level smoother on CG P3 64^3
     (untrained network: the kernels do the same work); dg-p3-32: FP64 vmults of
-    the headline DG P3 32^3 workload with kernel variant `variant`."""
+    the headline DG P3 32^3 workload with kernel variant `variant`.  For the
+    cg-* cases `variant` sets the kernel of the FP32 operator (e.g. 8: TF32
+    tensor cores per cube)."""
     import torch
     import simplexfem as sf
     out = {"case": name}
@@ -744,6 +747,8 @@ def run_case(name, reps=3, variant=0):
         mesh = sf.Mesh(n, jitter=JITTER, seed=0)
         for prec in ("fp64", "fp32"):
             op = sf.Operator(mesh, p, "cg", prec)
+            if variant and prec == "fp32":
+                op.set_kernel_variant(variant)
             x = torch.rand(op.m(), dtype=op.dtype, device="cuda")
             y = op.initialize_dof_vector()
             for _ in range(reps):
