@@ -569,15 +569,8 @@ __device__ __forceinline__ void load_cell(const DGProblem<T>& pr, int64_t c, Cel
 // staged src rows, then reuse those rows for the coalesced write-out, so the
 // CTA needs no separate result rows (less shared memory, more CTAs per SM).
 // BQ (NC == 1): block-major traces (dg_trace_blk_kernel), staged as [QN][BS].
-// XW (BQ only): compact rows per warp for neighbours outside the CTA's cells.
-// Once a thread's neighbour ids have arrived (they are requested before the
-// staging), it issues cp.async copies of each such neighbour's face values
-// (in this cell's face-node order) and traces into the next free row of its
-// warp (a warp prefix sum numbers them); the copies land while the CTA
-// finishes staging and computes the cell term.  Faces past XW rows read the
-// neighbour from global memory as before.
 template <int P, int NC, bool MASS, int BS, typename T, int MINB = (BS == 64 ? 6 : 1), bool ALIAS = false,
-          bool BQ = false, int XW = 0>
+          bool BQ = false>
 __global__ void __launch_bounds__(BS, MINB) dg_apply_kernel(const __grid_constant__ DGBatch<T> batch,
                                                             int64_t n_blocks) {
   using O = gen::Ops<P>;
@@ -587,9 +580,6 @@ __global__ void __launch_bounds__(BS, MINB) dg_apply_kernel(const __grid_constan
   T* su = reinterpret_cast<T*>(smem_raw);  // [BS][US]  src rows
   T* sq = su + BS * S::US;                 // [BS][QS]  published traces
   T* sy = ALIAS ? su : sq + BS * S::QS;    // [BS][US]  results
-  static_assert(XW == 0 || (BQ && NC == 1), "cross-block rows are for scalar block-major problems");
-  constexpr int XROW = O::NF + O::NFQ;
-  T* sx = (ALIAS ? sq + BS * S::QS : sy + BS * S::US) + (threadIdx.x >> 5) * XW * XROW;  // [XW][XROW] of this warp
   for (int64_t blk = blockIdx.x; blk < n_blocks; blk += gridDim.x) {
     const int pi = find_problem(batch, blk);
     const DGProblem<T>& pr = batch.p[pi];
@@ -604,47 +594,13 @@ __global__ void __launch_bounds__(BS, MINB) dg_apply_kernel(const __grid_constan
     stage_in<S::U, S::US, BS>(su, pr.src + c0 * S::U, nloc);
     if constexpr (BQ) stage_q_blk<S::QN, BS>(sq, pr.Q, c0, nloc);
     else stage_in<S::QN, S::QS, BS>(sq, pr.Q + c0 * S::QN, nloc);
-    int slot[4] = {-1, -1, -1, -1};
-    if constexpr (XW > 0) {
-      int cross = 0;
-      if (t < nloc) {
-#pragma unroll
-        for (int f = 0; f < 4; ++f) {
-          const int64_t lc = int64_t(d.nb[f]) - c0;
-          if (d.nb[f] >= 0 && (lc < 0 || lc >= nloc)) cross |= 1 << f;
-        }
-      }
-      const int cnt = __popc(cross), lane = t & 31;
-      int incl = cnt;
-#pragma unroll
-      for (int o = 1; o < 32; o <<= 1) {
-        const int v = __shfl_up_sync(0xffffffffu, incl, o);
-        if (lane >= o) incl += v;
-      }
-      int base = incl - cnt;
-#pragma unroll
-      for (int f = 0; f < 4; ++f) {
-        if ((cross >> f & 1) && base < XW) {
-          slot[f] = base;
-          T* dst = sx + base * XROW;
-          const T* un = pr.src + int64_t(d.nb[f]) * O::K;
-#pragma unroll
-          for (int i = 0; i < O::NF; ++i) cp_async_elem(dst + i, un + O::fn_runtime(d.nbf[f], i));
-#pragma unroll
-          for (int m = 0; m < O::NFQ; ++m)
-            cp_async_elem(dst + O::NF + m, q_blk_ptr<S::QN>(pr.Q, d.nb[f], d.nbf[f] * O::NFQ + m));
-        }
-        base += (cross >> f) & 1;
-      }
-      cp_async_commit();
-    }
     __syncthreads();
     const T* qs = BQ ? sq + t : sq + t * S::QS;  // this cell's traces
     if (ALIAS) {
       T y[O::K];
       if (t < nloc) {
-        dg_cell_component<P, NC, MASS, true, T, (XW > 0), BQ, BS>(pr, c0, 0, su + t * S::US, qs, su, sq, nloc, d.G,
-                                                                   d.sf, d.md, d.nb, d.nbf, y, sx, &slot);
+        dg_cell_component<P, NC, MASS, true, T, false, BQ, BS>(pr, c0, 0, su + t * S::US, qs, su, sq, nloc, d.G,
+                                                                d.sf, d.md, d.nb, d.nbf, y);
       }
       __syncthreads();  // every thread is done with the staged src rows
       if (t < nloc) {
@@ -655,8 +611,8 @@ __global__ void __launch_bounds__(BS, MINB) dg_apply_kernel(const __grid_constan
 #pragma unroll 1
       for (int comp = 0; comp < NC; ++comp) {
         T y[O::K];
-        dg_cell_component<P, NC, MASS, true, T, (XW > 0), BQ, BS>(pr, c0, comp, su + t * S::US, qs, su, sq, nloc,
-                                                                   d.G, d.sf, d.md, d.nb, d.nbf, y, sx, &slot);
+        dg_cell_component<P, NC, MASS, true, T, false, BQ, BS>(pr, c0, comp, su + t * S::US, qs, su, sq, nloc,
+                                                                d.G, d.sf, d.md, d.nb, d.nbf, y);
 #pragma unroll
         for (int i = 0; i < O::K; ++i) sy[t * S::US + comp * O::K + i] = y[i];
       }

@@ -1114,7 +1114,7 @@ class DGOperator final : public Operator {
     kern<<<unsigned(grid), kQB, S::SMEM, s>>>(b, n_blocks, status);
   }
 
-  template <int P, int NC, bool MASS, int BS, int MINB = (BS == 64 ? 6 : 1), bool ALIAS = false, int XW = 0>
+  template <int P, int NC, bool MASS, int BS, int MINB = (BS == 64 ? 6 : 1), bool ALIAS = false>
   static void run_cell(const DGProblem<T>* probs, int n, cudaStream_t s, int what, int* status) {
     using S = DGShape<P, NC>;
     int64_t n_blocks = 0;
@@ -1122,12 +1122,9 @@ class DGOperator final : public Operator {
     const size_t sm_trace = size_t(BS) * (S::US + S::QS) * sizeof(T);
     // scalar problems: block-major traces (no shared memory in the trace pass)
     constexpr bool BQ = NC == 1;
-    constexpr int XWC = BQ ? XW : 0;
-    const size_t sm_apply = (size_t(BS) * ((ALIAS ? 1 : 2) * S::US + S::QS) +
-                             size_t(BS / 32) * XWC * (gen::Ops<P>::NF + gen::Ops<P>::NFQ)) *
-                            sizeof(T);
+    const size_t sm_apply = size_t(BS) * ((ALIAS ? 1 : 2) * S::US + S::QS) * sizeof(T);
     static std::atomic<uint64_t> conf_t{0}, conf_a{0};
-    auto apply = dg_apply_kernel<P, NC, MASS, BS, T, MINB, ALIAS, BQ, XWC>;
+    auto apply = dg_apply_kernel<P, NC, MASS, BS, T, MINB, ALIAS, BQ>;
     opt_in_smem(apply, sm_apply, conf_a);
     if (what != 2) {
       if constexpr (BQ) {
