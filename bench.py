@@ -41,10 +41,11 @@ for p in (os.path.join(ROOT, "simplex-benchmarks_b200"), os.path.join(ROOT, "ora
 N_HEX, DEGREE, JITTER = 32, 3, 0.1
 METRIC = "vmult DoF/s (FP64 vs mixed); Poisson solve time to 1e-8 (MG vs learned)"
 WORKLOAD = "DG SIPG Poisson vmult, P3 on 32^3 x 6 Kuhn tets (196,608 cells, 3,932,160 DoFs), jitter 0.1h"
-# DRAM bytes (read + written) of one dg_apply_kernel<3,1,false,128,double> launch
-# on this workload: dram__bytes.sum.per_second x gpu__time_duration.sum of an ncu
-# capture (profiles/dg_apply_kernel_p3_fp64_32cube.md)
-APPLY_TRAFFIC_BYTES = 101.9e6
+# DRAM bytes (read + written) of one launch of the apply kernel on this
+# workload: dram__bytes_read.sum + dram__bytes_write.sum of an ncu capture
+# (profiles/dg_apply_kernel_p3_fp64_32cube.md)
+APPLY_KERNEL = "dg_apply_kernel<3,1,false,128,double,1,false,true>"
+APPLY_TRAFFIC_BYTES = 100.57e6
 
 
 def parse():
@@ -694,7 +695,7 @@ def run_ours(args):
                     "how": "fem_op_vmult_host over `steps` host vectors (pinned), copies of consecutive "
                            "vectors overlapped with the apply; one vector at a time on one stream: "
                            f"{e2e_serial_value:.4g} DoF/s"},
-            "roofline": {"bound": "hbm", "kernel": "dg_apply_kernel<3,1,false,128,double>",
+            "roofline": {"bound": "hbm", "kernel": APPLY_KERNEL,
                          "achieved": achieved_gbs, "peak": hbm, "unit": "GB/s",
                          "frac": achieved_gbs / hbm, "traffic": APPLY_TRAFFIC_BYTES,
                          "note": f"algorithmic bytes of one vmult ({alg_bytes:.4g} B) over the apply kernel's "
@@ -703,7 +704,7 @@ def run_ours(args):
             "fp64": {"achieved_tflops": flops / (vm_ms / 1e3) / 1e12, "peak_tflops_dgemm": fp64_peak,
                      "frac": (flops / (vm_ms / 1e3) / 1e12) / fp64_peak if fp64_peak else None,
                      "flops_per_vmult": flops},
-            "kernels_ms": {"dg_trace_kernel": statistics.mean(t_trace), "dg_apply_kernel": apply_ms,
+            "kernels_ms": {"dg_trace_tma_kernel": statistics.mean(t_trace), "dg_apply_kernel": apply_ms,
                            "vmult": vm_ms},
             "extra": {"fp32_value": value32, "fp32_ms_per_step": sum(t32) / args.steps},
             "solve": solve,

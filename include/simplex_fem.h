@@ -202,7 +202,7 @@ int fem_op_vmult_host(fem_op* op, int32_t n, void* const* dst_host, const void* 
  * through it shares the one library-owned array.  The array is held on every
  * GPU that loads the library, until exit, whether or not the call is used.
  * Operators needing more scratch are rejected with FEM_ERR_ARG (DG P3 FP64:
- * up to 87,381 cells).  All calls share the array, so calls that overlap on
+ * up to 87,296 cells).  All calls share the array, so calls that overlap on
  * the GPU race; order them on one stream.  Each call outside stream capture
  * looks up the array's device address; a call under capture reuses the last
  * one, so make one call on the device before capturing. */

@@ -16,7 +16,8 @@
 // operator's.  Creating the operator still allocates its tables.
 //
 // Limits and rules:
-//   - at most kStaticScratchBytes (16 MiB) of scratch: DG P3 FP64 up to 87,381
+//   - at most kStaticScratchBytes (16 MiB) of scratch (traces of whole 128-cell
+//     blocks): DG P3 FP64 up to 87,296
 //     cells (e.g. 24^3 x 6 = 82,944); larger problems are rejected with FEM_ERR_ARG;
 //   - every call shares the one array and leaves its contents behind; the
 //     scratch is fully written before it is read in each call, so nothing has

@@ -285,6 +285,8 @@ def test_dg_kernel_variants_config2_full_size(cuda, precision):
         op.set_kernel_variant(v)
         err = rel_l2(run_product(op, x), ref)
         assert err <= TOL[precision], (v, err)
+    # the bulk-copy trace pass of the scalar forms reports no bounded-wait timeout
+    assert op.status() == 0
 
 
 @pytest.mark.parametrize("kind", ["dg", "helmholtz"])
