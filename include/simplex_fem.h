@@ -239,8 +239,9 @@ int fem_csr_spmv(int64_t n_rows, const int64_t* row_ptr, const int32_t* col, con
 /* Algorithmic work of one vmult: flops and bytes of the fused kernels. */
 int fem_op_work(const fem_op* op, double* flops, double* bytes);
 /* Device-side status of the operator's kernels since the last call, then
- * cleared: bit 0 = a tensor-core kernel gave up on a bounded wait (that
- * vmult's result is invalid).  Synchronises with the device.  No counterpart
+ * cleared: bit 0 = a kernel gave up on a bounded wait (a tensor-core CG
+ * kernel, or the bulk-copy trace pass of a DG / Helmholtz operator); that
+ * vmult's result is invalid.  Synchronises with the device.  No counterpart
  * in the reference (its kernels have no bounded waits). */
 int fem_op_status(fem_op* op, int32_t* status);
 
