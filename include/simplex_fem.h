@@ -87,8 +87,7 @@ typedef struct fem_op_params {
                               cell, 2 thread per Kuhn hex (6 tets, one atomic per distinct
                               DoF), 3 CTA per 4x4x4-hex Morton cube (stores for cube-interior
                               DoFs); each falls back to the next simpler form where the mesh
-                              lacks the pattern; default P1 3 (FP64) / 2 (FP32), P2 3, P3 3
-                              (FP32) / 1 (FP64);
+                              lacks the pattern; default P1 3 (FP64) / 2 (FP32), P2 3, P3 3;
                               4: FP32 CG on the TF32 tensor cores (tcgen05 kind::tf32, cell
                               operator as one [128 cells x K] x [K x 6K] product; ~1e-3
                               relative accuracy, for multigrid levels); CG 5, 6, 7: the cube

@@ -19,6 +19,32 @@
 
 namespace sfem {
 
+// L1 cache policies of the cube kernels' loads: the tables every cube reads
+// (tet maps, reduce schedules) are kept (evict_last); the per-cube metric is
+// read once and not allocated in L1, so it does not push the tables out.
+__device__ __forceinline__ uint4 ld_keep(const uint4* p) {
+  uint4 v;
+  asm("ld.global.nc.L1::evict_last.v4.u32 {%0, %1, %2, %3}, [%4];"
+      : "=r"(v.x), "=r"(v.y), "=r"(v.z), "=r"(v.w)
+      : "l"(p));
+  return v;
+}
+__device__ __forceinline__ uint32_t ld_keep(const uint32_t* p) {
+  uint32_t v;
+  asm("ld.global.nc.L1::evict_last.u32 %0, [%1];" : "=r"(v) : "l"(p));
+  return v;
+}
+__device__ __forceinline__ double ld_stream(const double* p) {
+  double v;
+  asm("ld.global.nc.L1::no_allocate.f64 %0, [%1];" : "=d"(v) : "l"(p));
+  return v;
+}
+__device__ __forceinline__ float ld_stream(const float* p) {
+  float v;
+  asm("ld.global.nc.L1::no_allocate.f32 %0, [%1];" : "=f"(v) : "l"(p));
+  return v;
+}
+
 // G = |det J| J^-1 J^-T stored as (00, 11, 22, 01, 02, 12); w_b = sum_a G_ab g_a
 template <int KQ, typename T>
 __device__ __forceinline__ void apply_metric(const T (&G)[6], const T* g, T* w) {
@@ -238,23 +264,25 @@ __global__ void __launch_bounds__(BS) cg_hex_kernel(int64_t n_hex, const int32_t
 // DoF reduction of one cube (cube kernels): thread t sums the contributions of
 // its reduce slots n = 384 r + t from the per-tet result rows yr, in the order
 // of its cslot8 steps, and writes each DoF once (store for cube-interior DoFs,
-// atomic on the cube surface).  bd: the cube's row of bdof.
+// atomic on the cube surface).  bd: the cube's row of bdof; codes (when not
+// null): the same row's entries of this thread, already in registers.
 template <typename T, int NB>
 __device__ __forceinline__ void cube_reduce(int t, const int32_t* __restrict__ bd, const uint32_t* __restrict__ ritem,
-                                            const int16_t* __restrict__ cslot8, const T* yr, T* __restrict__ dst) {
+                                            const int16_t* __restrict__ cslot8, const T* yr, T* __restrict__ dst,
+                                            const int32_t (*codes)[(NB + 383) / 384] = nullptr) {
   constexpr int NJ = (NB + 383) / 384;
-#pragma unroll 1
+#pragma unroll
   for (int r = 0; r < NJ; ++r) {
     const int n = 384 * r + t;
     if (n >= NB) break;
-    const int32_t code = __ldg(bd + n);
+    const int32_t code = codes ? (*codes)[r] : __ldg(bd + n);
     if (code < 0) continue;
-    const uint32_t item = __ldg(ritem + n);
+    const uint32_t item = ld_keep(ritem + n);
     const uint4* grp = reinterpret_cast<const uint4*>(cslot8) + (item >> 8);
     const int steps = int(item & 0xFFu);  // per lane; the same for every lane in schedule 1
     T sum = T(0);
     for (int q = 0; 8 * q < steps; ++q) {
-      const uint4 w = __ldg(grp + 32 * q);
+      const uint4 w = ld_keep(grp + 32 * q);
       const uint32_t wv[4] = {w.x, w.y, w.z, w.w};
 #pragma unroll
       for (int h = 0; h < 8; ++h)
@@ -310,6 +338,14 @@ template <int P, typename T>
 __host__ __device__ constexpr bool cube_metric_smem() {
   return (P == 3 && sizeof(T) == 4) || (P == 1 && sizeof(T) == 8);
 }
+// Whether the reduction takes the cube's DoF codes from registers (one more
+// array of NJ codes kept across the iteration) instead of reloading them:
+// measured on B200, P3 FP32 64^3 130 -> 112 us; P2 FP64, capped at 56
+// registers for three CTAs per SM, spills and slows down (390 -> 404 us).
+template <int P, typename T>
+__host__ __device__ constexpr bool cube_codes_in_registers() {
+  return !(P == 2 && sizeof(T) == 8);
+}
 
 template <int P, typename T, int NB, int KP>
 __global__ void __launch_bounds__(384, P <= 2 ? 3 : (sizeof(T) == 4 ? 2 : 1))
@@ -321,6 +357,7 @@ __global__ void __launch_bounds__(384, P <= 2 ? 3 : (sizeof(T) == 4 ? 2 : 1))
   constexpr int KV = (K + 7) / 8 * 8;
   constexpr int NJ = (NB + 383) / 384;  // cube DoFs gathered per thread
   constexpr bool GS = cube_metric_smem<P, T>();
+  constexpr bool RC = cube_codes_in_registers<P, T>();
   extern __shared__ __align__(16) unsigned char smem_cube[];
   T* sg = reinterpret_cast<T*>(smem_cube);  // GS: [6][384] metric of the cube
   T* ubuf = sg + (GS ? 6 * 384 : 0);        // [2][NB]
@@ -374,11 +411,11 @@ __global__ void __launch_bounds__(384, P <= 2 ? 3 : (sizeof(T) == 4 ? 2 : 1))
   // !GS: the metric of cube bq into registers
   auto load_geo = [&](int64_t bq, T (&G)[6]) {
 #pragma unroll
-    for (int k = 0; k < 6; ++k) G[k] = bq < n_blocks ? __ldg(geo + k * n_cells + bq * 384 + t) : T(0);
+    for (int k = 0; k < 6; ++k) G[k] = bq < n_blocks ? ld_stream(geo + k * n_cells + bq * 384 + t) : T(0);
   };
 
   int64_t b = blockIdx.x;
-  int32_t code_cur[NJ], code_nxt[NJ];
+  int32_t code_cur[NJ], code_nxt[NJ], code_nn[NJ];  // DoF codes of cubes k, k+1, k+2
   T Gc[6], Gn[6];
   load_codes(b, code_cur);
   issue_gather(code_cur, 0, b < n_blocks);
@@ -390,9 +427,7 @@ __global__ void __launch_bounds__(384, P <= 2 ? 3 : (sizeof(T) == 4 ? 2 : 1))
     const bool more = b + stride < n_blocks;
     // gather of the next cube, codes of the one after (and !GS: metric of the next)
     issue_gather(code_nxt, buf ^ 1, more);
-#pragma unroll
-    for (int q = 0; q < NJ; ++q) code_cur[q] = code_nxt[q];
-    load_codes(b + 2 * stride, code_nxt);
+    load_codes(b + 2 * stride, code_nn);
     if (!GS) load_geo(b + stride, Gn);
     asm volatile("cp.async.wait_group 1;" ::: "memory");  // this cube's gather (GS: and metric)
     __syncthreads();
@@ -405,7 +440,7 @@ __global__ void __launch_bounds__(384, P <= 2 ? 3 : (sizeof(T) == 4 ? 2 : 1))
       int ti[KV];
 #pragma unroll
       for (int q = 0; q < KV / 8; ++q) {
-        const uint4 w = __ldg(tm + 384 * q);
+        const uint4 w = ld_keep(tm + 384 * q);
         const uint32_t wv[4] = {w.x, w.y, w.z, w.w};
 #pragma unroll
         for (int h = 0; h < 4; ++h) {
@@ -422,7 +457,12 @@ __global__ void __launch_bounds__(384, P <= 2 ? 3 : (sizeof(T) == 4 ? 2 : 1))
     }
     __syncthreads();
     if (GS) issue_geo(b + stride);  // every thread has read this cube's metric
-    cube_reduce<T, NB>(t, bdof + b * NB, ritem, cslot8, yr, dst);
+    cube_reduce<T, NB>(t, bdof + b * NB, ritem, cslot8, yr, dst, RC ? &code_cur : nullptr);
+#pragma unroll
+    for (int q = 0; q < NJ; ++q) {
+      code_cur[q] = code_nxt[q];
+      code_nxt[q] = code_nn[q];
+    }
     if (!GS) {
 #pragma unroll
       for (int k6 = 0; k6 < 6; ++k6) Gc[k6] = Gn[k6];

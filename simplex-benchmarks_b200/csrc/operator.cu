@@ -693,14 +693,15 @@ class CGOperator final : public Operator {
     }
     if (v == 0) {
       constexpr int64_t kFill = 2 * 148;
-      v = cfg.degree == 1 ? (sizeof(T) == 8 ? 3 : 2) : cfg.degree == 2 ? 3 : (sizeof(T) == 4 ? 3 : 1);
+      // measured on B200: P3 FP64 64^3 cube 181 against 191 us per cell
+      v = cfg.degree == 1 ? (sizeof(T) == 8 ? 3 : 2) : 3;
       if (v == 3 && n_blocks < kFill) v = 2;
       if (v == 2 && n_hex < kFill * kHexBS) v = 1;
     }
     // cube reduce schedule: variants 5, 6, 7 pick one; variant 3 takes the
     // one measured fastest on B200 (FP64 P1 and P2: bank-scheduled with
-    // uniform steps, 155 against 165 us and 396 against 415 us on 128^3;
-    // FP32: contribution order)
+    // uniform steps, 144 against 157 us and 380 against 380-413 us on 128^3;
+    // FP32 and P3: contribution order)
     int sched = v >= 5 ? v - 5 : (sizeof(T) == 8 && cfg.degree <= 2 ? 1 : 0);
     if (v >= 5) v = 3;
     if (v == 3 && cube_NB) {
