@@ -20,8 +20,9 @@
 namespace sfem {
 
 // L1 cache policies of the cube kernels' loads: the tables every cube reads
-// (tet maps, reduce schedules) are kept (evict_last); the per-cube metric is
-// read once and not allocated in L1, so it does not push the tables out.
+// (tet maps, reduce schedules) are kept (evict_last); the per-cube metric and
+// DoF codes are read once and not allocated in L1, so they do not push the
+// tables out.
 __device__ __forceinline__ uint4 ld_keep(const uint4* p) {
   uint4 v;
   asm("ld.global.nc.L1::evict_last.v4.u32 {%0, %1, %2, %3}, [%4];"
@@ -37,6 +38,11 @@ __device__ __forceinline__ uint32_t ld_keep(const uint32_t* p) {
 __device__ __forceinline__ double ld_stream(const double* p) {
   double v;
   asm("ld.global.nc.L1::no_allocate.f64 %0, [%1];" : "=d"(v) : "l"(p));
+  return v;
+}
+__device__ __forceinline__ int32_t ld_stream(const int32_t* p) {
+  int32_t v;
+  asm("ld.global.nc.L1::no_allocate.s32 %0, [%1];" : "=r"(v) : "l"(p));
   return v;
 }
 __device__ __forceinline__ float ld_stream(const float* p) {
@@ -338,17 +344,17 @@ template <int P, typename T>
 __host__ __device__ constexpr bool cube_metric_smem() {
   return (P == 3 && sizeof(T) == 4) || (P == 1 && sizeof(T) == 8);
 }
-// Whether the reduction takes the cube's DoF codes from registers (one more
-// array of NJ codes kept across the iteration) instead of reloading them:
-// measured on B200, P3 FP32 64^3 130 -> 112 us; P2 FP64, capped at 56
-// registers for three CTAs per SM, spills and slows down (390 -> 404 us).
+// Resident CTAs per SM of the cube kernel (its register cap).  P2 FP64 runs
+// two CTAs with up to 85 registers: with three (56 registers) the DoF codes
+// of the current cube spill (measured on B200, 128^3: 356 us with two CTAs,
+// 404 us with three).
 template <int P, typename T>
-__host__ __device__ constexpr bool cube_codes_in_registers() {
-  return !(P == 2 && sizeof(T) == 8);
+__host__ __device__ constexpr int cube_min_ctas() {
+  return (P == 2 && sizeof(T) == 8) ? 2 : P <= 2 ? 3 : (sizeof(T) == 4 ? 2 : 1);
 }
 
 template <int P, typename T, int NB, int KP>
-__global__ void __launch_bounds__(384, P <= 2 ? 3 : (sizeof(T) == 4 ? 2 : 1))
+__global__ void __launch_bounds__(384, cube_min_ctas<P, T>())
     cg_cube_pipe_kernel(int64_t n_blocks, const int16_t* __restrict__ tmapv, const int32_t* __restrict__ bdof,
                         const uint32_t* __restrict__ ritem, const int16_t* __restrict__ cslot8,
                         const T* __restrict__ geo, const T* __restrict__ src, T* __restrict__ dst, int64_t n_constrained, const int32_t* __restrict__ constrained) {
@@ -357,7 +363,6 @@ __global__ void __launch_bounds__(384, P <= 2 ? 3 : (sizeof(T) == 4 ? 2 : 1))
   constexpr int KV = (K + 7) / 8 * 8;
   constexpr int NJ = (NB + 383) / 384;  // cube DoFs gathered per thread
   constexpr bool GS = cube_metric_smem<P, T>();
-  constexpr bool RC = cube_codes_in_registers<P, T>();
   extern __shared__ __align__(16) unsigned char smem_cube[];
   T* sg = reinterpret_cast<T*>(smem_cube);  // GS: [6][384] metric of the cube
   T* ubuf = sg + (GS ? 6 * 384 : 0);        // [2][NB]
@@ -374,7 +379,7 @@ __global__ void __launch_bounds__(384, P <= 2 ? 3 : (sizeof(T) == 4 ? 2 : 1))
 #pragma unroll
     for (int q = 0; q < NJ; ++q) {
       const int j = t + 384 * q;
-      code[q] = (b < n_blocks && j < NB) ? __ldg(bdof + b * NB + j) : -1;
+      code[q] = (b < n_blocks && j < NB) ? ld_stream(bdof + b * NB + j) : -1;
     }
   };
   // cp.async of this thread's share of cube DoF values into buffer `buf`
@@ -457,7 +462,7 @@ __global__ void __launch_bounds__(384, P <= 2 ? 3 : (sizeof(T) == 4 ? 2 : 1))
     }
     __syncthreads();
     if (GS) issue_geo(b + stride);  // every thread has read this cube's metric
-    cube_reduce<T, NB>(t, bdof + b * NB, ritem, cslot8, yr, dst, RC ? &code_cur : nullptr);
+    cube_reduce<T, NB>(t, bdof + b * NB, ritem, cslot8, yr, dst, &code_cur);
 #pragma unroll
     for (int q = 0; q < NJ; ++q) {
       code_cur[q] = code_nxt[q];
