@@ -275,7 +275,8 @@ __global__ void __launch_bounds__(BS) cg_hex_kernel(int64_t n_hex, const int32_t
 template <typename T, int NB>
 __device__ __forceinline__ void cube_reduce(int t, const int32_t* __restrict__ bd, const uint32_t* __restrict__ ritem,
                                             const int16_t* __restrict__ cslot8, const T* yr, T* __restrict__ dst,
-                                            const int32_t (*codes)[(NB + 383) / 384] = nullptr) {
+                                            const int32_t (*codes)[(NB + 383) / 384] = nullptr,
+                                            const uint32_t (*items)[(NB + 383) / 384] = nullptr) {
   constexpr int NJ = (NB + 383) / 384;
 #pragma unroll
   for (int r = 0; r < NJ; ++r) {
@@ -283,7 +284,7 @@ __device__ __forceinline__ void cube_reduce(int t, const int32_t* __restrict__ b
     if (n >= NB) break;
     const int32_t code = codes ? (*codes)[r] : __ldg(bd + n);
     if (code < 0) continue;
-    const uint32_t item = ld_keep(ritem + n);
+    const uint32_t item = items ? (*items)[r] : ld_keep(ritem + n);
     const uint4* grp = reinterpret_cast<const uint4*>(cslot8) + (item >> 8);
     const int steps = int(item & 0xFFu);  // per lane; the same for every lane in schedule 1
     T sum = T(0);
@@ -421,6 +422,17 @@ __global__ void __launch_bounds__(384, cube_min_ctas<P, T>())
 
   int64_t b = blockIdx.x;
   int32_t code_cur[NJ], code_nxt[NJ], code_nn[NJ];  // DoF codes of cubes k, k+1, k+2
+  // HOIST: the tet map and reduce items are the same for every cube; with two
+  // or fewer CTAs per SM there are registers to hold them across the loop
+  constexpr bool HOIST = cube_min_ctas<P, T>() <= 2;
+  uint4 tmv[KV / 8];
+  uint32_t items[NJ];
+  if (HOIST) {
+#pragma unroll
+    for (int q = 0; q < KV / 8; ++q) tmv[q] = ld_keep(reinterpret_cast<const uint4*>(tmapv) + t + 384 * q);
+#pragma unroll
+    for (int q = 0; q < NJ; ++q) items[q] = (384 * q + t < NB) ? ld_keep(ritem + 384 * q + t) : 0u;
+  }
   T Gc[6], Gn[6];
   load_codes(b, code_cur);
   issue_gather(code_cur, 0, b < n_blocks);
@@ -441,11 +453,11 @@ __global__ void __launch_bounds__(384, cube_min_ctas<P, T>())
 #pragma unroll
       for (int k6 = 0; k6 < 6; ++k6) G[k6] = GS ? sg[k6 * 384 + t] : Gc[k6];
       const T* ub = ubuf + buf * NB;
-      const uint4* tm = reinterpret_cast<const uint4*>(tmapv) + t;
+      const uint4* tm = reinterpret_cast<const uint4*>(tmapv) + t;  // unused when HOIST
       int ti[KV];
 #pragma unroll
       for (int q = 0; q < KV / 8; ++q) {
-        const uint4 w = ld_keep(tm + 384 * q);
+        const uint4 w = HOIST ? tmv[q] : ld_keep(tm + 384 * q);
         const uint32_t wv[4] = {w.x, w.y, w.z, w.w};
 #pragma unroll
         for (int h = 0; h < 4; ++h) {
@@ -462,7 +474,7 @@ __global__ void __launch_bounds__(384, cube_min_ctas<P, T>())
     }
     __syncthreads();
     if (GS) issue_geo(b + stride);  // every thread has read this cube's metric
-    cube_reduce<T, NB>(t, bdof + b * NB, ritem, cslot8, yr, dst, &code_cur);
+    cube_reduce<T, NB>(t, bdof + b * NB, ritem, cslot8, yr, dst, &code_cur, HOIST ? &items : nullptr);
 #pragma unroll
     for (int q = 0; q < NJ; ++q) {
       code_cur[q] = code_nxt[q];
