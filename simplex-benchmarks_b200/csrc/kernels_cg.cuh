@@ -22,32 +22,34 @@ namespace sfem {
 // L1 cache policies of the cube kernels' loads: the tables every cube reads
 // (tet maps, reduce schedules) are kept (evict_last); the per-cube metric and
 // DoF codes are read once and not allocated in L1, so they do not push the
-// tables out.
+// tables out.  The asm is volatile and every call sits under an explicit
+// bounds test: a non-volatile asm load counts as side-effect free, and the
+// compiler may then execute it ahead of the test that guards its address.
 __device__ __forceinline__ uint4 ld_keep(const uint4* p) {
   uint4 v;
-  asm("ld.global.nc.L1::evict_last.v4.u32 {%0, %1, %2, %3}, [%4];"
+  asm volatile("ld.global.nc.L1::evict_last.v4.u32 {%0, %1, %2, %3}, [%4];"
       : "=r"(v.x), "=r"(v.y), "=r"(v.z), "=r"(v.w)
       : "l"(p));
   return v;
 }
 __device__ __forceinline__ uint32_t ld_keep(const uint32_t* p) {
   uint32_t v;
-  asm("ld.global.nc.L1::evict_last.u32 %0, [%1];" : "=r"(v) : "l"(p));
+  asm volatile("ld.global.nc.L1::evict_last.u32 %0, [%1];" : "=r"(v) : "l"(p));
   return v;
 }
 __device__ __forceinline__ double ld_stream(const double* p) {
   double v;
-  asm("ld.global.nc.L1::no_allocate.f64 %0, [%1];" : "=d"(v) : "l"(p));
+  asm volatile("ld.global.nc.L1::no_allocate.f64 %0, [%1];" : "=d"(v) : "l"(p));
   return v;
 }
 __device__ __forceinline__ int32_t ld_stream(const int32_t* p) {
   int32_t v;
-  asm("ld.global.nc.L1::no_allocate.s32 %0, [%1];" : "=r"(v) : "l"(p));
+  asm volatile("ld.global.nc.L1::no_allocate.s32 %0, [%1];" : "=r"(v) : "l"(p));
   return v;
 }
 __device__ __forceinline__ float ld_stream(const float* p) {
   float v;
-  asm("ld.global.nc.L1::no_allocate.f32 %0, [%1];" : "=f"(v) : "l"(p));
+  asm volatile("ld.global.nc.L1::no_allocate.f32 %0, [%1];" : "=f"(v) : "l"(p));
   return v;
 }
 
@@ -270,19 +272,49 @@ __global__ void __launch_bounds__(BS) cg_hex_kernel(int64_t n_hex, const int32_t
 // DoF reduction of one cube (cube kernels): thread t sums the contributions of
 // its reduce slots n = 384 r + t from the per-tet result rows yr, in the order
 // of its cslot8 steps, and writes each DoF once (store for cube-interior DoFs,
-// atomic on the cube surface).  bd: the cube's row of bdof; codes (when not
-// null): the same row's entries of this thread, already in registers.
+// atomic on the cube surface).  bd: the cube's row of bdof.
 template <typename T, int NB>
 __device__ __forceinline__ void cube_reduce(int t, const int32_t* __restrict__ bd, const uint32_t* __restrict__ ritem,
-                                            const int16_t* __restrict__ cslot8, const T* yr, T* __restrict__ dst,
-                                            const int32_t (*codes)[(NB + 383) / 384] = nullptr,
-                                            const uint32_t (*items)[(NB + 383) / 384] = nullptr) {
+                                            const int16_t* __restrict__ cslot8, const T* yr, T* __restrict__ dst) {
+  constexpr int NJ = (NB + 383) / 384;
+#pragma unroll 1
+  for (int r = 0; r < NJ; ++r) {
+    const int n = 384 * r + t;
+    if (n >= NB) break;
+    const int32_t code = __ldg(bd + n);
+    if (code < 0) continue;
+    const uint32_t item = __ldg(ritem + n);
+    const uint4* grp = reinterpret_cast<const uint4*>(cslot8) + (item >> 8);
+    const int steps = int(item & 0xFFu);  // per lane; the same for every lane in schedule 1
+    T sum = T(0);
+    for (int q = 0; 8 * q < steps; ++q) {
+      const uint4 w = __ldg(grp + 32 * q);
+      const uint32_t wv[4] = {w.x, w.y, w.z, w.w};
+#pragma unroll
+      for (int h = 0; h < 8; ++h)
+        if (8 * q + h < steps) sum += yr[(h & 1) ? (wv[h >> 1] >> 16) : (wv[h >> 1] & 0xFFFFu)];
+    }
+    const int32_t g = code & 0x3FFFFFFF;
+    if (code & 0x40000000) dst[g] = sum;
+    else atomicAdd(dst + g, sum);
+  }
+}
+
+// The same reduction for cg_cube_pipe_kernel: the cube's DoF codes of this
+// thread come from registers; reduce items from registers when `items` is
+// given (else loaded, kept in L1), schedules loaded with L1::evict_last.
+template <typename T, int NB>
+__device__ __forceinline__ void cube_reduce_regs(int t, const int32_t (&codes)[(NB + 383) / 384],
+                                                 const uint32_t* __restrict__ ritem,
+                                                 const uint32_t (*items)[(NB + 383) / 384],
+                                                 const int16_t* __restrict__ cslot8, const T* yr,
+                                                 T* __restrict__ dst) {
   constexpr int NJ = (NB + 383) / 384;
 #pragma unroll
   for (int r = 0; r < NJ; ++r) {
     const int n = 384 * r + t;
     if (n >= NB) break;
-    const int32_t code = codes ? (*codes)[r] : __ldg(bd + n);
+    const int32_t code = codes[r];
     if (code < 0) continue;
     const uint32_t item = items ? (*items)[r] : ld_keep(ritem + n);
     const uint4* grp = reinterpret_cast<const uint4*>(cslot8) + (item >> 8);
@@ -380,7 +412,8 @@ __global__ void __launch_bounds__(384, cube_min_ctas<P, T>())
 #pragma unroll
     for (int q = 0; q < NJ; ++q) {
       const int j = t + 384 * q;
-      code[q] = (b < n_blocks && j < NB) ? ld_stream(bdof + b * NB + j) : -1;
+      code[q] = -1;
+      if (b < n_blocks && j < NB) code[q] = ld_stream(bdof + b * NB + j);
     }
   };
   // cp.async of this thread's share of cube DoF values into buffer `buf`
@@ -417,7 +450,10 @@ __global__ void __launch_bounds__(384, cube_min_ctas<P, T>())
   // !GS: the metric of cube bq into registers
   auto load_geo = [&](int64_t bq, T (&G)[6]) {
 #pragma unroll
-    for (int k = 0; k < 6; ++k) G[k] = bq < n_blocks ? ld_stream(geo + k * n_cells + bq * 384 + t) : T(0);
+    for (int k = 0; k < 6; ++k) {
+      G[k] = T(0);
+      if (bq < n_blocks) G[k] = ld_stream(geo + k * n_cells + bq * 384 + t);
+    }
   };
 
   int64_t b = blockIdx.x;
@@ -431,7 +467,10 @@ __global__ void __launch_bounds__(384, cube_min_ctas<P, T>())
 #pragma unroll
     for (int q = 0; q < KV / 8; ++q) tmv[q] = ld_keep(reinterpret_cast<const uint4*>(tmapv) + t + 384 * q);
 #pragma unroll
-    for (int q = 0; q < NJ; ++q) items[q] = (384 * q + t < NB) ? ld_keep(ritem + 384 * q + t) : 0u;
+    for (int q = 0; q < NJ; ++q) {
+      items[q] = 0u;
+      if (384 * q + t < NB) items[q] = ld_keep(ritem + 384 * q + t);
+    }
   }
   T Gc[6], Gn[6];
   load_codes(b, code_cur);
@@ -474,7 +513,7 @@ __global__ void __launch_bounds__(384, cube_min_ctas<P, T>())
     }
     __syncthreads();
     if (GS) issue_geo(b + stride);  // every thread has read this cube's metric
-    cube_reduce<T, NB>(t, bdof + b * NB, ritem, cslot8, yr, dst, &code_cur, HOIST ? &items : nullptr);
+    cube_reduce_regs<T, NB>(t, code_cur, ritem, HOIST ? &items : nullptr, cslot8, yr, dst);
 #pragma unroll
     for (int q = 0; q < NJ; ++q) {
       code_cur[q] = code_nxt[q];

@@ -693,7 +693,7 @@ class CGOperator final : public Operator {
     }
     if (v == 0) {
       constexpr int64_t kFill = 2 * 148;
-      // measured on B200: P3 FP64 64^3 cube 181 against 191 us per cell
+      // measured on B200: P3 FP64 64^3 cube 171 against 190 us per cell
       v = cfg.degree == 1 ? (sizeof(T) == 8 ? 3 : 2) : 3;
       if (v == 3 && n_blocks < kFill) v = 2;
       if (v == 2 && n_hex < kFill * kHexBS) v = 1;
