@@ -469,9 +469,6 @@ __device__ __forceinline__ void dg_cell_component(const DGProblem<T>& pr, int64_
     for (int i = 0; i < K; ++i) y[i] = T(0);
     if (MASS) O::massP(uu, md, y);
   }
-  // staged cross-block rows were copied by this thread's own cp.async
-  // instructions: the cell term above covered their latency
-  if constexpr (XS) cp_async_wait_all();
 #pragma unroll
   for (int f = 0; f < 4; ++f) {
     T cf[3];
