@@ -27,6 +27,7 @@ const char* last_error();
 #include <cuda_runtime.h>
 
 #include <atomic>
+#include <mutex>
 
 #include "../../include/simplex_fem.h"
 #define SFEM_CUDA(call)                                                                   \
@@ -37,13 +38,25 @@ const char* last_error();
   } while (0)
 
 namespace sfem {
-// Per-device one-time set-up (kernel attributes are set per device): returns
-// true the first time it is called with `mask` while device `dev` is current.
-// Bit d of the mask stands for device d; ordinals of 64 and above are refused.
-inline bool first_use_on_device(std::atomic<uint64_t>& mask, int dev) {
+inline std::mutex& device_setup_mutex() {
+  static std::mutex m;
+  return m;
+}
+// Per-device one-time set-up (kernel attributes are set per device): runs
+// init() the first time it is called with `mask` while device `dev` is
+// current.  Bit d of the mask stands for device d (ordinals of 64 and above
+// are refused); it is set only after init() has finished, and concurrent
+// first callers wait for it, so no caller launches a kernel before its
+// attributes are in place.  If init() throws, the device stays unconfigured.
+template <class F>
+inline void once_per_device(std::atomic<uint64_t>& mask, int dev, F&& init) {
   if (dev < 0 || dev >= 64) throw Error(FEM_ERR_INTERNAL, "device ordinal out of range (0..63)");
   const uint64_t bit = uint64_t(1) << dev;
-  return (mask.fetch_or(bit) & bit) == 0;
+  if (mask.load(std::memory_order_acquire) & bit) return;
+  std::lock_guard<std::mutex> lock(device_setup_mutex());
+  if (mask.load(std::memory_order_relaxed) & bit) return;
+  init();
+  mask.fetch_or(bit, std::memory_order_release);
 }
 }  // namespace sfem
 #endif

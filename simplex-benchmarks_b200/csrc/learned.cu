@@ -36,8 +36,9 @@ void launch_tc(int64_t n, const int32_t* dofs, const float* feat, const float* w
   auto kern = mlp_tc_kernel<MODE, T>;
   int dev = 0, sms = 0;
   SFEM_CUDA(cudaGetDevice(&dev));
-  if (first_use_on_device(configured, dev))
+  once_per_device(configured, dev, [&] {
     SFEM_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, tc::SMEM_BYTES));
+  });
   SFEM_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
   const int64_t tiles = (n + tc::TILE - 1) / tc::TILE;
   const int64_t groups = (tiles + tc::GROUPS - 1) / tc::GROUPS;
@@ -156,8 +157,9 @@ double LearnedSmoother::gradient(const float* X, const float* Y, int n, float* g
   const int smem = 2 * NP * int(sizeof(float));
   int dev = 0;
   SFEM_CUDA(cudaGetDevice(&dev));
-  if (first_use_on_device(configured, dev))
+  once_per_device(configured, dev, [&] {
     SFEM_CUDA(cudaFuncSetAttribute(mlp_grad_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
+  });
   SFEM_CUDA(cudaMemsetAsync(grad, 0, sizeof(float) * NP, s));
   SFEM_CUDA(cudaMemsetAsync(loss_.p, 0, sizeof(float), s));
   const int grid = std::min((n + 127) / 128, 148 * 2);

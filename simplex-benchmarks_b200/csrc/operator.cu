@@ -1077,8 +1077,9 @@ class DGOperator final : public Operator {
   static void opt_in_smem(K kernel, size_t bytes, std::atomic<uint64_t>& configured) {
     int dev = 0;
     SFEM_CUDA(cudaGetDevice(&dev));
-    if (first_use_on_device(configured, dev))
+    once_per_device(configured, dev, [&] {
       SFEM_CUDA(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, int(bytes)));
+    });
   }
 
   // The bulk-copy trace pass needs every copy 16-byte aligned and a whole
@@ -1103,14 +1104,14 @@ class DGOperator final : public Operator {
     static int grid_per_dev[64] = {};
     int dev = 0;
     SFEM_CUDA(cudaGetDevice(&dev));
-    if (first_use_on_device(conf, dev)) {
+    once_per_device(conf, dev, [&] {
       SFEM_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, S::SMEM));
       int sms = 0, occ = 0;
       SFEM_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
       SFEM_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, kern, kQB, S::SMEM));
       SFEM_REQUIRE(occ > 0, FEM_ERR_CUDA, "DG trace pass does not fit on an SM");
       grid_per_dev[dev] = sms * occ;
-    }
+    });
     const int64_t grid = std::max<int64_t>(1, std::min<int64_t>(n_blocks, grid_per_dev[dev]));
     kern<<<unsigned(grid), kQB, S::SMEM, s>>>(b, n_blocks, status);
   }
