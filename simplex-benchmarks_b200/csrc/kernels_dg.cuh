@@ -10,8 +10,11 @@
 //
 // Element-centric, deterministic, no atomics: every cell writes its own DoF
 // block once.  Two passes per vmult:
-//   A (dg_trace_kernel):  q_f = 2|F| d_n u on face f at the P_{p-1} face nodes,
-//                         for all 4 faces of every cell (published in Q);
+//   A (trace pass):       q_f = 2|F| d_n u on face f at the P_{p-1} face nodes,
+//                         for all 4 faces of every cell (published in Q):
+//                         dg_trace_tma_kernel (scalar problems, bulk copies),
+//                         dg_trace_blk_kernel (scalar, unaligned vectors),
+//                         dg_trace_kernel (3-component problems);
 //   B (dg_apply_kernel):  cell term + the complete face terms of the cell's 4
 //                         faces, reading the neighbour's face values from src and
 //                         its published q from Q.
@@ -21,11 +24,14 @@
 // that bucket key, and the element-centric form removes the scatter.
 //
 // Memory: one thread per cell, BS cells per CTA.  A CTA's cells are
-// contiguous, so their DoF blocks (and their Q blocks) are one contiguous
-// range: it is copied into shared memory with coalesced loads, into rows
-// padded to an odd number of words (conflict-free per-thread reads), and the
-// results leave the same way.  Neighbours inside the CTA are read from shared
-// memory, the others from L2.
+// contiguous, so their DoF blocks are one contiguous range: it is copied into
+// shared memory with coalesced loads, into rows padded to an odd number of
+// words (conflict-free per-thread reads), and the results leave the same way.
+// Q is [cell][4][NC][NFQ] rows for 3-component problems and block-major for
+// scalar ones (see dg_trace_blk_kernel).  Neighbours inside the CTA are read
+// from shared memory, the others from L2.  Each cell's geometry and neighbour
+// ids are requested before its block is staged, so their latency overlaps
+// the staging rather than the compute.
 //
 // Geometry per cell (structure of arrays, n_cells stride):
 //   [0..5]  G = |det J| J^-1 J^-T           (00,11,22,01,02,12)
