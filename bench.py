@@ -44,7 +44,7 @@ WORKLOAD = "DG SIPG Poisson vmult, P3 on 32^3 x 6 Kuhn tets (196,608 cells, 3,93
 # DRAM bytes (read + written) of one launch of the apply kernel on this
 # workload: dram__bytes_read.sum + dram__bytes_write.sum of an ncu capture
 # (profiles/dg_apply_kernel_p3_fp64_32cube.md)
-APPLY_KERNEL = "dg_apply_kernel<3,1,false,128,double,1,false,true>"
+APPLY_KERNEL = "dg_apply_kernel<3,1,false,128,double,1,false,true,1>"
 APPLY_TRAFFIC_BYTES = 100.57e6
 
 

@@ -109,6 +109,16 @@ __device__ __forceinline__ void cp_async_elem(T* smem, const T* gmem) {
 __device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
 __device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_group 0;\n" ::: "memory"); }
 
+// Programmatic dependent launch (sm_90 and later).  The trace pass lets the
+// apply pass of the same vmult launch while it still runs; the apply pass
+// does the work that does not read the traces (its geometry, neighbour ids,
+// src rows, optionally the cell term) and then waits for the whole trace grid
+// - its completion and the visibility of its stores - before it reads Q.  A
+// kernel launched without the programmatic-serialization attribute returns
+// from the wait at once.
+__device__ __forceinline__ void pdl_trigger() { asm volatile("griddepcontrol.launch_dependents;" ::: "memory"); }
+__device__ __forceinline__ void pdl_wait() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
+
 // J^-1 (2|F_f| n_f) for local face f
 template <typename T>
 __device__ __forceinline__ void face_cf(const T (&G)[6], int f, T (&cf)[3]) {
@@ -234,6 +244,7 @@ __global__ void __launch_bounds__(kQB) dg_trace_blk_kernel(const __grid_constant
                                                            int64_t n_blocks) {
   using O = gen::Ops<P>;
   constexpr int K = O::K, KQ = O::KQ, NFQ = O::NFQ, QN = 4 * NFQ;
+  pdl_trigger();
   for (int64_t blk = blockIdx.x; blk < n_blocks; blk += gridDim.x) {
     const int pi = find_problem(batch, blk);
     const DGProblem<T>& pr = batch.p[pi];
@@ -330,6 +341,7 @@ __global__ void __launch_bounds__(kQB) dg_trace_tma_kernel(const __grid_constant
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     for (int64_t k = 0; k < NS && k < mine; ++k) issue(k);
   }
+  pdl_trigger();
   __syncthreads();
   int64_t done = 0;  // blocks whose stage wait completed
   bool ok = true;
@@ -437,44 +449,42 @@ __global__ void __launch_bounds__(BS) dg_trace_kernel(const __grid_constant__ DG
   }
 }
 
-// Own-cell terms plus face terms for one component.  u and qm come from the
-// staged rows of this cell (`us`, `qs`); HAVE_NB reads the neighbour traces
-// (from shared memory when the neighbour is in this CTA, rows su/sq),
-// otherwise they are zero (diagonal).
-// XS: `xs` points at this cell's staged cross-block neighbour data, one row
-// of XROW values per face slot (slot[f] < 0: not staged): the neighbour's
-// face values already in this cell's face-node order, then its traces.
-// BQ (scalar): the traces are block-major, staged as [QN][BSQ] (qs = sq + this
-// cell's local index), and a neighbour in another block is read from pr.Q in
-// the block-major layout.
-template <int P, int NC, bool MASS, bool HAVE_NB, typename T, bool XS = false, bool BQ = false, int BSQ = 1>
-__device__ __forceinline__ void dg_cell_component(const DGProblem<T>& pr, int64_t c0, int comp,
-                                                  const T* us, const T* qs, const T* su, const T* sq, int nloc,
-                                                  const T (&G)[6], const T (&sf)[4], T md,
-                                                  const int32_t (&nb)[4], const int (&nbf)[4],
-                                                  T (&y)[gen::Ops<P>::K], const T* xs = nullptr,
-                                                  const int (*slot)[4] = nullptr) {
+// Cell term of one component: h = MQ (G grad u) (the gradient test before
+// the face terms) and y = m|J| MP u (or 0).  u: the component's K values.
+template <int P, bool MASS, typename T>
+__device__ __forceinline__ void dg_cell_term(const T* u, const T (&G)[6], T md, T (&h)[3 * gen::Ops<P>::KQ],
+                                             T (&y)[gen::Ops<P>::K]) {
+  using O = gen::Ops<P>;
+  constexpr int K = O::K, KQ = O::KQ;
+  T uu[K];
+#pragma unroll
+  for (int i = 0; i < K; ++i) uu[i] = u[i];
+  T g[3 * KQ];
+  O::grad(uu, g);
+  T w[3 * KQ];
+  apply_metric<KQ>(G, g, w);
+#pragma unroll
+  for (int a = 0; a < 3; ++a) O::massQ(w + a * KQ, h + a * KQ);
+#pragma unroll
+  for (int i = 0; i < K; ++i) y[i] = T(0);
+  if (MASS) O::massP(uu, md, y);
+}
+
+// The four faces' terms of one component added to the cell term (h, y),
+// then y += D^T h.  Arguments as for dg_cell_component.
+template <int P, int NC, bool HAVE_NB, typename T, bool XS = false, bool BQ = false, int BSQ = 1>
+__device__ __forceinline__ void dg_face_terms(const DGProblem<T>& pr, int64_t c0, int comp,
+                                              const T* us, const T* qs, const T* su, const T* sq, int nloc,
+                                              const T (&G)[6], const T (&sf)[4],
+                                              const int32_t (&nb)[4], const int (&nbf)[4],
+                                              T (&h)[3 * gen::Ops<P>::KQ], T (&y)[gen::Ops<P>::K],
+                                              const T* xs = nullptr, const int (*slot)[4] = nullptr) {
   using O = gen::Ops<P>;
   using S = DGShape<P, NC>;
   constexpr int K = O::K, KQ = O::KQ, NF = O::NF, NFQ = O::NFQ;
   static_assert(!BQ || NC == 1, "block-major traces are for scalar problems");
   constexpr int QST = BQ ? BSQ : 1;  // stride of a cell's consecutive traces in shared memory
   const T* u = us + comp * K;
-  T h[3 * KQ];
-  {
-    T uu[K];
-#pragma unroll
-    for (int i = 0; i < K; ++i) uu[i] = u[i];
-    T g[3 * KQ];
-    O::grad(uu, g);
-    T w[3 * KQ];
-    apply_metric<KQ>(G, g, w);
-#pragma unroll
-    for (int a = 0; a < 3; ++a) O::massQ(w + a * KQ, h + a * KQ);
-#pragma unroll
-    for (int i = 0; i < K; ++i) y[i] = T(0);
-    if (MASS) O::massP(uu, md, y);
-  }
 #pragma unroll
   for (int f = 0; f < 4; ++f) {
     T cf[3];
@@ -545,6 +555,29 @@ __device__ __forceinline__ void dg_cell_component(const DGProblem<T>& pr, int64_
   O::gradT(h, y);
 }
 
+// Own-cell terms plus face terms for one component.  u and qm come from the
+// staged rows of this cell (`us`, `qs`); HAVE_NB reads the neighbour traces
+// (from shared memory when the neighbour is in this CTA, rows su/sq),
+// otherwise they are zero (diagonal).
+// XS: `xs` points at this cell's staged cross-block neighbour data, one row
+// of XROW values per face slot (slot[f] < 0: not staged): the neighbour's
+// face values already in this cell's face-node order, then its traces.
+// BQ (scalar): the traces are block-major, staged as [QN][BSQ] (qs = sq + this
+// cell's local index), and a neighbour in another block is read from pr.Q in
+// the block-major layout.
+template <int P, int NC, bool MASS, bool HAVE_NB, typename T, bool XS = false, bool BQ = false, int BSQ = 1>
+__device__ __forceinline__ void dg_cell_component(const DGProblem<T>& pr, int64_t c0, int comp,
+                                                  const T* us, const T* qs, const T* su, const T* sq, int nloc,
+                                                  const T (&G)[6], const T (&sf)[4], T md,
+                                                  const int32_t (&nb)[4], const int (&nbf)[4],
+                                                  T (&y)[gen::Ops<P>::K], const T* xs = nullptr,
+                                                  const int (*slot)[4] = nullptr) {
+  T h[3 * gen::Ops<P>::KQ];
+  dg_cell_term<P, MASS>(us + comp * gen::Ops<P>::K, G, md, h, y);
+  dg_face_terms<P, NC, HAVE_NB, T, XS, BQ, BSQ>(pr, c0, comp, us, qs, su, sq, nloc, G, sf, nb, nbf, h, y, xs,
+                                                slot);
+}
+
 template <typename T>
 struct CellData {
   T G[6], sf[4], md;
@@ -572,8 +605,12 @@ __device__ __forceinline__ void load_cell(const DGProblem<T>& pr, int64_t c, Cel
 // staged src rows, then reuse those rows for the coalesced write-out, so the
 // CTA needs no separate result rows (less shared memory, more CTAs per SM).
 // BQ (NC == 1): block-major traces (dg_trace_blk_kernel), staged as [QN][BS].
+// PDLM: launched as a programmatic dependent of the trace pass.  1: the
+// geometry and the src rows are loaded before the wait for the trace grid;
+// 2 (scalar, block-major traces): the cell term is computed before the wait
+// as well, and the traces are staged after it.
 template <int P, int NC, bool MASS, int BS, typename T, int MINB = (BS == 64 ? 6 : 1), bool ALIAS = false,
-          bool BQ = false>
+          bool BQ = false, int PDLM = 0>
 __global__ void __launch_bounds__(BS, MINB) dg_apply_kernel(const __grid_constant__ DGBatch<T> batch,
                                                             int64_t n_blocks) {
   using O = gen::Ops<P>;
@@ -595,6 +632,27 @@ __global__ void __launch_bounds__(BS, MINB) dg_apply_kernel(const __grid_constan
     if (t < nloc) load_cell<MASS>(pr, c0 + t, d);
     __syncthreads();
     stage_in<S::U, S::US, BS>(su, pr.src + c0 * S::U, nloc);
+    if constexpr (PDLM == 2) {
+      static_assert(NC == 1 && BQ, "cell term before the wait: scalar problems, block-major traces");
+      __syncthreads();  // src rows staged
+      T h[3 * O::KQ], y[O::K];
+      if (t < nloc) dg_cell_term<P, MASS>(su + t * S::US, d.G, d.md, h, y);
+      pdl_wait();
+      stage_q_blk<S::QN, BS>(sq, pr.Q, c0, nloc);
+      __syncthreads();
+      if (t < nloc)
+        dg_face_terms<P, NC, true, T, false, BQ, BS>(pr, c0, 0, su + t * S::US, sq + t, su, sq, nloc, d.G, d.sf, d.nb,
+                                                     d.nbf, h, y);
+      if (ALIAS) __syncthreads();  // every thread is done with the staged src rows
+      if (t < nloc) {
+#pragma unroll
+        for (int i = 0; i < O::K; ++i) sy[t * S::US + i] = y[i];
+      }
+      __syncthreads();
+      stage_out<S::U, S::US, BS>(pr.dst + c0 * S::U, sy, nloc);
+      continue;
+    }
+    if constexpr (PDLM == 1) pdl_wait();
     if constexpr (BQ) stage_q_blk<S::QN, BS>(sq, pr.Q, c0, nloc);
     else stage_in<S::QN, S::QS, BS>(sq, pr.Q + c0 * S::QN, nloc);
     __syncthreads();
