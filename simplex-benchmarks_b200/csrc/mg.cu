@@ -165,6 +165,73 @@ __global__ void __launch_bounds__(128) transfer_restrict_add_k(int64_t nf, const
   }
 }
 
+// p-transfers on one mesh (every cell is its own parent, one embedding
+// matrix): the matrix travels as a kernel parameter, so the unrolled
+// products read it as constant-bank operands instead of issuing a load per
+// entry (the forms above spend most of their time waiting on those loads).
+template <int KF, int KC>
+struct XferMat {
+  double m[KF * KC];
+};
+
+template <typename T, int KF, int KC>
+__global__ void __launch_bounds__(128) transfer_p_prolongate_k(int64_t n, const uint32_t* __restrict__ owner,
+                                                               const __grid_constant__ XferMat<KF, KC> M,
+                                                               const int32_t* __restrict__ fdofs,
+                                                               const int32_t* __restrict__ cdofs,
+                                                               const T* __restrict__ xc, T* __restrict__ xf) {
+  const int64_t c = blockIdx.x * int64_t(blockDim.x) + threadIdx.x;
+  if (c >= n) return;
+  const uint32_t ow = __ldg(owner + c);
+  if (!ow) return;
+  double xl[KC];
+#pragma unroll
+  for (int j = 0; j < KC; ++j) {
+    const int32_t g = __ldg(cdofs + j * n + c);
+    xl[j] = g >= 0 ? double(__ldg(xc + g)) : 0.0;
+  }
+#pragma unroll
+  for (int i = 0; i < KF; ++i) {
+    if (!((ow >> i) & 1u)) continue;
+    const int32_t g = __ldg(fdofs + i * n + c);
+    if (g < 0) continue;
+    double acc = 0.0;
+#pragma unroll
+    for (int j = 0; j < KC; ++j) acc += M.m[i * KC + j] * xl[j];
+    xf[g] += T(acc);
+  }
+}
+
+template <typename T, int KF, int KC>
+__global__ void __launch_bounds__(128) transfer_p_restrict_k(int64_t n, const uint32_t* __restrict__ owner,
+                                                             const __grid_constant__ XferMat<KF, KC> M,
+                                                             const int32_t* __restrict__ fdofs,
+                                                             const int32_t* __restrict__ cdofs,
+                                                             const T* __restrict__ xf, T* __restrict__ xc) {
+  const int64_t c = blockIdx.x * int64_t(blockDim.x) + threadIdx.x;
+  if (c >= n) return;
+  const uint32_t ow = __ldg(owner + c);
+  if (!ow) return;
+  double rl[KF];
+#pragma unroll
+  for (int i = 0; i < KF; ++i) {
+    rl[i] = 0.0;
+    if ((ow >> i) & 1u) {
+      const int32_t g = __ldg(fdofs + i * n + c);
+      if (g >= 0) rl[i] = double(__ldg(xf + g));
+    }
+  }
+#pragma unroll
+  for (int j = 0; j < KC; ++j) {
+    const int32_t g = __ldg(cdofs + j * n + c);
+    if (g < 0) continue;
+    double acc = 0.0;
+#pragma unroll
+    for (int i = 0; i < KF; ++i) acc += M.m[i * KC + j] * rl[i];
+    if (acc != 0.0) atomicAdd(xc + g, T(acc));
+  }
+}
+
 // DG p-transfer on one mesh: cell-local embedding P_{p-1} -> P_p, no sharing
 // (DG/cells_batched/application_phc.cc:3396-3475 builds the same two-level
 // transfer with MGTwoLevelTransfer on FE_SimplexDGP).  Layout [cell][K].
@@ -454,6 +521,7 @@ class MultigridImpl final : public Multigrid {
     DevBuf<uint8_t> mat_id;
     DevBuf<uint32_t> owner;
     DevBuf<double> mats;
+    std::vector<double> mats_host;  // p-transfers: the embedding matrix as a kernel parameter
   };
   std::vector<std::unique_ptr<Mesh>> meshes_;  // owned h-level meshes
   std::vector<Level> levels_;
@@ -572,6 +640,7 @@ class MultigridImpl final : public Multigrid {
       F.mat_id.upload(th.mat_id);
       F.owner.upload(th.owner);
       F.mats.upload(th.mats);
+      if (F.mesh == Cl.mesh) F.mats_host = th.mats;
     }
     partial_.alloc(kReduceBlocks);
     scal_.alloc(1);
@@ -757,6 +826,14 @@ class MultigridImpl final : public Multigrid {
     SFEM_CUDA(cudaGetLastError());
   }
 
+  template <int KF, int KC>
+  static XferMat<KF, KC> xfer_mat(const Level& F) {
+    SFEM_REQUIRE(F.mats_host.size() == size_t(KF) * KC, FEM_ERR_INTERNAL, "multigrid: p-transfer matrix shape");
+    XferMat<KF, KC> M;
+    std::memcpy(M.m, F.mats_host.data(), sizeof(M.m));
+    return M;
+  }
+
   void prolongate_add(int l, void* dst, const void* src, cudaStream_t s) override {
     Level& F = levels_.at(l);
     SFEM_REQUIRE(l > 0, FEM_ERR_ARG, "prolongate: level must be >= 1");
@@ -774,6 +851,18 @@ class MultigridImpl final : public Multigrid {
       SFEM_CUDA(cudaGetLastError());
       return;
     }
+#define SFEM_PXFER(KF_, KC_)                                                                               \
+  if (F.Kf == KF_ && F.Kc == KC_) {                                                                        \
+    transfer_p_prolongate_k<T, KF_, KC_><<<grid, 128, 0, s>>>(                                             \
+        F.op->n_cells, F.owner.p, xfer_mat<KF_, KC_>(F), F.op->device_dof_table(), Cl.op->device_dof_table(), \
+        static_cast<const T*>(src), static_cast<T*>(dst));                                                 \
+    SFEM_CUDA(cudaGetLastError());                                                                        \
+    return;                                                                                               \
+  }
+    if (!F.mats_host.empty()) {
+      SFEM_PXFER(20, 10) SFEM_PXFER(10, 4)
+    }
+#undef SFEM_PXFER
 #define SFEM_XFER(KF_, KC_)                                                                                \
   if (F.Kf == KF_ && F.Kc == KC_) {                                                                        \
     transfer_prolongate_add_k<T, KF_, KC_><<<grid, 128, 0, s>>>(                                           \
@@ -807,6 +896,18 @@ class MultigridImpl final : public Multigrid {
       SFEM_CUDA(cudaGetLastError());
       return;
     }
+#define SFEM_PXFER(KF_, KC_)                                                                               \
+  if (F.Kf == KF_ && F.Kc == KC_) {                                                                        \
+    transfer_p_restrict_k<T, KF_, KC_><<<grid, 128, 0, s>>>(                                               \
+        F.op->n_cells, F.owner.p, xfer_mat<KF_, KC_>(F), F.op->device_dof_table(), Cl.op->device_dof_table(), \
+        static_cast<const T*>(src), static_cast<T*>(dst));                                                 \
+    SFEM_CUDA(cudaGetLastError());                                                                        \
+    return;                                                                                               \
+  }
+    if (!F.mats_host.empty()) {
+      SFEM_PXFER(20, 10) SFEM_PXFER(10, 4)
+    }
+#undef SFEM_PXFER
 #define SFEM_XFER(KF_, KC_)                                                                                \
   if (F.Kf == KF_ && F.Kc == KC_) {                                                                        \
     transfer_restrict_add_k<T, KF_, KC_><<<grid, 128, 0, s>>>(                                             \
