@@ -813,8 +813,7 @@ class MultigridImpl final : public Multigrid {
       cheb_first_zero<T><<<g, 256, 0, s>>>(m, T(1.0 / theta), L.inv_diag.p, b, L.d.p, x);
     } else {
       L.op->vmult(L.t.p, x, s);
-      SFEM_CUDA(cudaMemsetAsync(L.d.p, 0, sizeof(T) * m, s));
-      cheb_step<T><<<g, 256, 0, s>>>(m, T(0), T(1.0 / theta), L.inv_diag.p, b, L.t.p, L.d.p, x);
+      cheb_step<T, true><<<g, 256, 0, s>>>(m, T(0), T(1.0 / theta), L.inv_diag.p, b, L.t.p, L.d.p, x);
     }
     for (int k = 1; k < params.smoother_degree; ++k) {
       const double rho_new = 1.0 / (2.0 * theta / delta - rho);
@@ -1066,7 +1065,17 @@ CGSolver::CGSolver(Operator& A, Preconditioner* M, bool flexible) : A_(A), M_(M)
   q_.alloc(m);
   if (flexible) zold_.alloc(m);
   partial_.alloc(kReduceBlocks + 1);
-  SFEM_CUDA(cudaMallocHost(&host_, sizeof(double)));
+  sc_.alloc(8);
+  SFEM_CUDA(cudaMallocHost(&host_, 2 * sizeof(double)));
+}
+
+CGSolver::~CGSolver() {
+  if (host_) cudaFreeHost(host_);
+}
+
+void CGSolver::dot_to(const double* x, const double* y, int slot, cudaStream_t s) {
+  vec_dot_partial<double><<<kReduceBlocks, kReduceThreads, 0, s>>>(A_.m, x, y, partial_.p);
+  reduce_partials<<<1, kReduceThreads, 0, s>>>(kReduceBlocks, partial_.p, sc_.p + slot);
 }
 
 double CGSolver::dot(const double* x, const double* y, cudaStream_t s) {
@@ -1101,12 +1110,22 @@ SolveInfo CGSolver::solve(double* x, const double* b, double rtol, int maxit, cu
   };
   precondition(z_.p, r_.p);
   SFEM_CUDA(cudaMemcpyAsync(p_.p, z_.p, sizeof(double) * m, cudaMemcpyDeviceToDevice, s));
-  double rz = dot(r_.p, z_.p, s);
+  // alpha and beta stay on the device: one host read per iteration, of
+  // (p,Ap) and (r,r) together, for the breakdown and convergence checks
+  constexpr int kPQ = 2, kRR = 3, kRZOLD = 4;
+  int cur = 0;  // slot of (r,z) of this iteration; 1 - cur: the next one
+  dot_to(r_.p, z_.p, cur, s);
   double prev_rn = info.r0;
   info.status = FEM_ERR_NOT_CONVERGED;
   for (int it = 1; it <= maxit; ++it) {
     A_.vmult(q_.p, p_.p, s);
-    const double pq = dot(p_.p, q_.p, s);
+    dot_to(p_.p, q_.p, kPQ, s);
+    cg_update_xr_dev<<<g, 256, 0, s>>>(m, sc_.p, cur, kPQ, p_.p, q_.p, x, r_.p);
+    dot_to(r_.p, r_.p, kRR, s);
+    SFEM_CUDA(cudaMemcpyAsync(host_, sc_.p + kPQ, 2 * sizeof(double), cudaMemcpyDeviceToHost, s));
+    SFEM_CUDA(cudaStreamSynchronize(s));
+    const double pq = host_[0];
+    rr = host_[1];
     if (!std::isfinite(pq)) {
       info.status = FEM_ERR_NONFINITE;
       info.iterations = it;
@@ -1117,9 +1136,6 @@ SolveInfo CGSolver::solve(double* x, const double* b, double rtol, int maxit, cu
       info.iterations = it;
       break;
     }
-    const double alpha = rz / pq;
-    cg_update_xr<<<g, 256, 0, s>>>(m, alpha, p_.p, q_.p, x, r_.p);
-    rr = dot(r_.p, r_.p, s);
     info.iterations = it;
     info.rn = std::sqrt(rr);
     if (!std::isfinite(rr)) {
@@ -1136,11 +1152,11 @@ SolveInfo CGSolver::solve(double* x, const double* b, double rtol, int maxit, cu
     prev_rn = info.rn;
     if (flexible_) SFEM_CUDA(cudaMemcpyAsync(zold_.p, z_.p, sizeof(double) * m, cudaMemcpyDeviceToDevice, s));
     precondition(z_.p, r_.p);
-    const double rz_new = dot(r_.p, z_.p, s);
-    double beta = rz_new / rz;
-    if (flexible_) beta = (rz_new - dot(r_.p, zold_.p, s)) / rz;
-    vec_axpby<double><<<g, 256, 0, s>>>(m, 1.0, z_.p, beta, p_.p);  // p = z + beta p
-    rz = rz_new;
+    dot_to(r_.p, z_.p, 1 - cur, s);
+    if (flexible_) dot_to(r_.p, zold_.p, kRZOLD, s);
+    // p = z + beta p, beta = (r,z)_new / (r,z), or ((r,z)_new - (r,z_old)) / (r,z)
+    cg_update_p_dev<<<g, 256, 0, s>>>(m, 1.0, sc_.p, 1 - cur, flexible_ ? kRZOLD : -1, cur, z_.p, p_.p);
+    cur = 1 - cur;
   }
   SFEM_CUDA(cudaGetLastError());
   return info;

@@ -97,15 +97,23 @@ class CGSolver {
  public:
   // flexible: Polak-Ribiere beta (for preconditioners that change between applications)
   CGSolver(Operator& A, Preconditioner* M, bool flexible);
+  ~CGSolver();
+  CGSolver(const CGSolver&) = delete;
+  CGSolver& operator=(const CGSolver&) = delete;
   SolveInfo solve(double* x, const double* b, double rtol, int maxit, cudaStream_t s);
   double dot(const double* x, const double* y, cudaStream_t s);
 
  private:
+  // (x, y) into the device scalar sc_[slot], no host synchronisation
+  void dot_to(const double* x, const double* y, int slot, cudaStream_t s);
   Operator& A_;
   Preconditioner* M_;
   bool flexible_;
   DevBuf<double> r_, z_, p_, q_, zold_, partial_;
-  double* host_ = nullptr;
+  // device scalars of the iteration: [0],[1] (r,z) of this and the next
+  // iteration (alternating), [2] (p,Ap), [3] (r,r), [4] (r,z_old)
+  DevBuf<double> sc_;
+  double* host_ = nullptr;  // pinned: (p,Ap), (r,r) read back once per iteration
 };
 
 class MGPreconditioner final : public Preconditioner {

@@ -82,12 +82,13 @@ __global__ void cheb_first_zero(int64_t n, T c, const T* __restrict__ invd, cons
   }
 }
 
-// Chebyshev step: d = f1 d + f2 P (b - t), x += d   (t = A x)
-template <typename T>
+// Chebyshev step: d = f1 d + f2 P (b - t), x += d   (t = A x); FIRST: the
+// first step from a nonzero x, d = f2 P (b - t) (d is not read)
+template <typename T, bool FIRST = false>
 __global__ void cheb_step(int64_t n, T f1, T f2, const T* __restrict__ invd, const T* __restrict__ b,
                           const T* __restrict__ t, T* __restrict__ d, T* __restrict__ x) {
   for (int64_t i = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; i < n; i += int64_t(gridDim.x) * blockDim.x) {
-    const T v = f1 * d[i] + f2 * invd[i] * (b[i] - t[i]);
+    const T v = (FIRST ? T(0) : f1 * d[i]) + f2 * invd[i] * (b[i] - t[i]);
     d[i] = v;
     x[i] += v;
   }
@@ -118,13 +119,27 @@ __global__ void dense_matvec(int n, const double* __restrict__ A, const T* __res
   if (lane == 0) y[warp] = T(acc);
 }
 
-// PCG update: x += alpha p, r -= alpha q
-static __global__ void cg_update_xr(int64_t n, double alpha, const double* __restrict__ p, const double* __restrict__ q,
-                             double* __restrict__ x, double* __restrict__ r) {
+// CG update with the step read on the device: alpha = sc[rz] / sc[pq];
+// nothing is updated unless sc[pq] is finite and positive (the host reads
+// sc[pq] after the step and reports the breakdown)
+static __global__ void cg_update_xr_dev(int64_t n, const double* __restrict__ sc, int rz, int pq,
+                                        const double* __restrict__ p, const double* __restrict__ q,
+                                        double* __restrict__ x, double* __restrict__ r) {
+  const double den = sc[pq];
+  if (!(den > 0) || !isfinite(den)) return;
+  const double alpha = sc[rz] / den;
   for (int64_t i = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; i < n; i += int64_t(gridDim.x) * blockDim.x) {
     x[i] += alpha * p[i];
     r[i] -= alpha * q[i];
   }
+}
+
+// p = a z + beta p with beta = (sc[num] - (sub >= 0 ? sc[sub] : 0)) / sc[den], read on the device
+static __global__ void cg_update_p_dev(int64_t n, double a, const double* __restrict__ sc, int num, int sub, int den,
+                                       const double* __restrict__ z, double* __restrict__ p) {
+  const double beta = (sub >= 0 ? sc[num] - sc[sub] : sc[num]) / sc[den];
+  for (int64_t i = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; i < n; i += int64_t(gridDim.x) * blockDim.x)
+    p[i] = a * z[i] + beta * p[i];
 }
 
 // x += (sc[0]/sc[1]) z  (step 0 unless sc[1] > 0); the ratio stays on the device
