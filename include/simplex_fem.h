@@ -348,7 +348,10 @@ int fem_mg_coarse_solve(fem_mg* mg, void* dst, const void* src, void* stream);
 /* ---- preconditioned CG ---------------------------------------------------
  * SolverCG (application_ph.cc:1949-1980) on an FP64 operator; stops when
  * ||r|| <= rtol ||b||.  status: FEM_OK, FEM_ERR_NOT_CONVERGED,
- * FEM_ERR_BREAKDOWN (p^T A p <= 0) or FEM_ERR_NONFINITE. */
+ * FEM_ERR_BREAKDOWN (p^T A p <= 0) or FEM_ERR_NONFINITE; on a breakdown or a
+ * non-finite p^T A p, x and r keep the previous iterate.  The step lengths
+ * stay on the device; the host reads p^T A p and r^T r back once per
+ * iteration (it synchronises with `stream` there). */
 enum { FEM_PRECOND_NONE = 0, FEM_PRECOND_JACOBI = 1, FEM_PRECOND_MG = 2 };
 typedef struct fem_solve_info {
   int32_t iterations;
