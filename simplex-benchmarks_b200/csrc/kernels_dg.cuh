@@ -18,6 +18,9 @@
 //   B (dg_apply_kernel):  cell term + the complete face terms of the cell's 4
 //                         faces, reading the neighbour's face values from src and
 //                         its published q from Q.
+// For scalar problems B is launched as a programmatic dependent of A: its
+// CTAs start while A's last blocks run, load what does not depend on A, and
+// wait for A's grid before they read Q (pdl_trigger / pdl_wait).
 // The reference instead sweeps faces in 576 (f_int,f_ext,o_int,o_ext) buckets
 // and scatters into both sides (DG/cells_batched/application.cc:1738-2431);
 // sorting every cell's vertices by global id removes the orientation part of
