@@ -61,7 +61,8 @@ def parse():
     ap.add_argument("--dd", action="store_true",
                     help="domain decomposition instead of replicas: one 32^3 x 6-tet DG P3 block per rank of a "
                          "32 x 32 x 32N mesh, halo exchange over NCCL every vmult")
-    ap.add_argument("--case", choices=["cg-p2-64", "cg-p3-64", "cg-p1-128", "cg-p2-128", "mlp-64", "dg-p3-32"],
+    ap.add_argument("--case", choices=["cg-p2-64", "cg-p3-64", "cg-p1-128", "cg-p2-128", "mlp-64", "dg-p3-32",
+                                       "solve-p3-64"],
                     help="run one small kernel workload (for profiling) instead of the benchmark")
     ap.add_argument("--variant", type=int, default=0,
                     help="kernel variant of --case dg-p3-32, or of the FP32 operator of a cg-* case (0: default)")
@@ -728,7 +729,9 @@ def run_case(name, reps=3, variant=0):
     (untrained network: the kernels do the same work); dg-p3-32: FP64 vmults of
     the headline DG P3 32^3 workload with kernel variant `variant`.  For the
     cg-* cases `variant` sets the kernel of the FP32 operator (e.g. 8: TF32
-    tensor cores per cube)."""
+    tensor cores per cube).  solve-p3-64: the kernel timeline of one mixed
+    MG-CG solve of the config-3 problem (CUPTI through torch.profiler): per
+    kernel its launches and device time, and the time between kernels."""
     import torch
     import simplexfem as sf
     out = {"case": name}
@@ -769,6 +772,52 @@ def run_case(name, reps=3, variant=0):
         torch.cuda.synchronize()
         out["finite"] = bool(torch.isfinite(x).all())
         out["timed_out"] = mlp.timed_out()
+    elif name == "solve-p3-64":
+        from torch.profiler import profile, ProfilerActivity
+        mesh = sf.Mesh(64)
+        op = sf.Operator(mesh, 3, "cg", "fp64")
+        b = sf.rhs(op, sf.sine_modes_rhs())
+        x = op.initialize_dof_vector()
+        mg = sf.Multigrid(op, precision="fp32", smoother_degree=3)
+        cg = sf.SolverCG(op, mg)
+        cg.solve(x, b, rtol=1e-8)  # warm-up (graph capture)
+        plain = []
+        for _ in range(reps):
+            x.zero_()
+            torch.cuda.synchronize()
+            t0 = time.perf_counter()
+            r = cg.solve(x, b, rtol=1e-8)
+            torch.cuda.synchronize()
+            plain.append(1e3 * (time.perf_counter() - t0))
+        x.zero_()
+        torch.cuda.synchronize()
+        with profile(activities=[ProfilerActivity.CUDA]) as prof:
+            r = cg.solve(x, b, rtol=1e-8)
+            torch.cuda.synchronize()
+        ev = sorted((e.time_range.start, e.time_range.end, e.name) for e in prof.events()
+                    if e.device_type == torch.autograd.DeviceType.CUDA)
+        busy, cur_s, cur_e = 0.0, None, None
+        for s0, e0, _ in ev:
+            if cur_e is None or s0 > cur_e:
+                if cur_e is not None:
+                    busy += cur_e - cur_s
+                cur_s, cur_e = s0, e0
+            else:
+                cur_e = max(cur_e, e0)
+        if cur_e is not None:
+            busy += cur_e - cur_s
+        span = (max(e for _, e, _ in ev) - ev[0][0]) if ev else 0.0
+        per = {}
+        for s0, e0, n in ev:
+            c, t = per.get(n, (0, 0.0))
+            per[n] = (c + 1, t + e0 - s0)
+        top = sorted(per.items(), key=lambda kv: -kv[1][1])[:20]
+        out.update({"iterations": r["iterations"], "solve_ms": [round(t, 2) for t in plain],
+                    "launches": len(ev), "span_us": round(span, 1), "busy_us": round(busy, 1),
+                    "gaps_us": round(span - busy, 1),
+                    "kernels": [{"name": n[:100], "launches": c, "us": round(t, 1),
+                                 "share_of_busy": round(t / busy, 3) if busy else None}
+                                for n, (c, t) in top]})
     else:
         raise SystemExit(f"unknown case {name}")
     print(json.dumps(out), flush=True)
