@@ -55,6 +55,29 @@ def test_embedding_reproduces_coarse_basis(tables, p):
         assert abs(vc @ coarse - vf @ fine) < 1e-13
 
 
+@pytest.mark.parametrize("p", [2, 3])
+def test_gradient_matrices_are_vertex_permutations_of_one(tables, p):
+    """D_a[m][i] = D_0[q(m)][p(i)]: swapping reference vertices 1 and a+1
+    (barycentric lattice components 1 and a+1) maps the x_0 derivative onto
+    the x_a derivative, and permutes the P_p and P_{p-1} nodes (p, q).  This
+    is the symmetry a per-direction split of the cell term relies on."""
+    d, dq = tables[p], tables[p - 1]
+    lat, latq = [tuple(x) for x in d["LATTICE"]], [tuple(x) for x in dq["LATTICE"]]
+    D = [[[float(x) for x in row] for row in Da] for Da in d["D"]]
+
+    def swap(t, a):
+        t = list(t)
+        t[1], t[a + 1] = t[a + 1], t[1]
+        return tuple(t)
+
+    for a in (1, 2):
+        perm = [lat.index(swap(x, a)) for x in lat]
+        permq = [latq.index(swap(x, a)) for x in latq]
+        for m in range(d["KQ"]):
+            for i in range(d["K"]):
+                assert D[a][m][i] == D[0][permq[m]][perm[i]]
+
+
 @pytest.mark.parametrize("p", [1, 2, 3])
 def test_face_node_lists_lie_on_faces(tables, p):
     lat = tables[p]["LATTICE"]
